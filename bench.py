@@ -1,0 +1,505 @@
+#!/usr/bin/env python
+"""Benchmark of the SL-BDF2 channel step (slchannel_b200) on B200s.
+
+Workload: slChannel's plain float64 SL-BDF2 step at 256^3 -- staggered MAC
+channel 4pi x 2pi x 2, tanh gamma = 2.0, Re_b = 2792.8 (nu = 1/2792.8), bulk
+velocity 1, triquintic (order 6), fixed dt = 0.01 -- from a seeded synthetic
+field: Poiseuille 1.5 z (2 - z) plus the curl of a seeded random vector
+potential (|k| <= 8, damped by z^2 (2-z)^2, u'_rms = 0.1), bulk-rescaled and
+projected; one BDF1 bootstrap step precedes the timed BDF2 steps.
+
+    python bench.py [--gpus N --steps K --warmup W]      # this implementation
+    python bench.py --impl reference [...]               # CPU reference arm
+
+Multi-GPU: the single-channel step does not shard (replicas only): each rank
+advances its own channel; value = total steps over all ranks / max rank time.
+
+One JSON line on rank 0 (see the fields below).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "SL steps/s at 256^3: mixed vs FP64 form at stated error; gather HBM GB/s"
+UNIT = "steps/s"
+LX, LY, LZ = 4 * math.pi, 2 * math.pi, 2.0
+GAMMA = 2.0
+RE_B = 2792.8
+DT = 0.01
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=256, help="grid points per direction")
+    ap.add_argument("--order", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0,
+                    help="CPU seconds the cpu_baseline sample aims for")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas: no collective on the data path)
+# ---------------------------------------------------------------------------
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def dist_init(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            import tempfile
+
+            fd, self.path = tempfile.mkstemp(prefix="slc_clocks_", suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                   "-lms", "200"]
+            if self.gpu_id is not None:
+                cmd += ["-i", str(self.gpu_id)]
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "power_w_max": max(power) if power else None, "reasons": sorted(reasons)}
+
+
+def gpu_smi_id(dev_index):
+    import torch
+
+    try:
+        p = torch.cuda.get_device_properties(dev_index)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in vis.split(",") if v.strip()]
+        return ids[dev_index] if dev_index < len(ids) else None
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def config(n, order, precision="fp64"):
+    return {
+        "grid": {"nx": n, "ny": n, "nz": n},
+        "domain": {"Lx": LX, "Ly": LY, "Lz": LZ, "stretching_type": "symmetric"},
+        "flow": {"Re": RE_B, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": GAMMA},
+        "boundary_conditions": {"top_wall": {"type": "dirichlet"}},
+        "initialization": {"type": "parabolic"},
+        "time": {"dt": DT, "dt_update_interval": 0},
+        "compute": {"device": "cuda"},
+        "sl": {"interp_order": order, "n_traj_iters": 2, "interp_dtype": precision},
+    }
+
+
+def initial_field(n, z_f, z_c, seed=0):
+    from slchannel_b200.fields import synthetic_channel_field
+
+    return synthetic_channel_field(n, n, n, LX, LY, LZ, z_f, z_c, urms=0.1, seed=seed)
+
+
+def build_flow(n, order, precision="fp64", seed=0):
+    import torch
+
+    from slchannel_b200.solver import SLChannelFlow
+    from slchannel_b200.utils import compute_bulk_velocity
+
+    flow = SLChannelFlow(config=config(n, order, precision))
+    u, v, w = initial_field(n, flow.z_f.cpu().numpy(), flow.z_c.cpu().numpy(), seed)
+    flow.set_state(*(torch.from_numpy(a) for a in (u, v, w)))
+    ub = float(compute_bulk_velocity(flow.u, flow.cell_vol_ratio, flow.total_volume))
+    flow.u *= 1.0 / ub
+    flow._save_and_project_initial()
+    flow.step_sl_bdf2(DT)  # BDF1 bootstrap; timed steps are BDF2
+    return flow
+
+
+def field_bytes(n):
+    u = (n + 1) * (n + 2) * (n + 2)
+    w = (n + 2) * (n + 2) * (n + 1)
+    return 8 * u, 8 * u, 8 * w, 8 * (n + 2) ** 3
+
+
+def sl_algorithmic(n, order):
+    """Per step, the fused trace+gather+BDF2 kernels (3 launches): compulsory
+    HBM bytes = read V^n, V^{n-1}, U* (9 ghost-shaped fields) + write u_hat
+    (3 interiors); FLOPs per arrival point both feet (FMA = 2): trace 3
+    trilinear sample points x (3 x 8-point samples + locate) ~ 3 x 100,
+    weights 2 x (3 x ~(5 order) products + order-6 z table), contraction
+    2 x 2 (O^3 + O^2 + O)."""
+    bu, bv, bw, _ = field_bytes(n)
+    n_u = n * n * n
+    n_w = n * n * (n - 1)
+    reads = 3 * (bu + bv + bw)
+    writes = 8 * (2 * n_u + n_w)
+    pts = 2 * n_u + n_w
+    contraction = 2 * (order**3 + order**2 + order)
+    weights = 3 * (4 * order) + 20
+    trace = 3 * 100
+    flops_pt = trace + 2 * (weights + contraction)
+    return reads + writes, flops_pt * pts, pts
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_per_point():
+    """DRAM bytes per arrival point of the fused trace+gather kernel, from the
+    ncu summary committed in profiles/ (line 'dram_bytes_per_point: X')."""
+    path = os.path.join(REPO, "profiles", "k_sl_bdf2_o6_fp64.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_point:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle port timed on this host's cores
+# ---------------------------------------------------------------------------
+
+def cpu_step_sample(n, order, budget_s, seed=0):
+    """Time the oracle (the CPU restatement of the reference's float64 path)
+    on a bounded sample of one 256^3 BDF2 step and extrapolate to a whole
+    step.  Returns (seconds per full step, description, threads)."""
+    import oracle.slbdf2 as O
+
+    z_f, z_c, dz_f, dz_c = O.generate_grid(GAMMA, n, LZ)
+    u, v, w = initial_field(n, z_f, z_c, seed)
+    ch = O.OracleChannel(n, n, n, LX, LY, LZ, GAMMA, 1.0 / RE_B, u, v, w, order=order, z_f=z_f, z_c=z_c)
+    adv = ch.sl
+    fb = {c: adv.fill(c, f) for c, f in zip("uvw", (ch.u, ch.v, ch.w))}
+    mid = fb  # U* = 2 V^n - V^{n-1} with V^{n-1} = V^n: the cost does not depend on the values
+    threads = O.max_threads()
+    # calibrate: seconds per arrival point for one component, both feet
+    nzi = {"u": n, "v": n, "w": n - 1}
+    probe = n * nzi["u"]  # one x-plane
+    t0 = time.perf_counter()
+    adv.advect_comp("u", fb["u"], mid, 2 * DT, 0, probe)
+    adv.advect_comp("u", fb["u"], mid, DT, 0, probe)
+    per_pt = (time.perf_counter() - t0) / probe
+    total_pts = sum(n * n * nzi[c] for c in "uvw")
+    # sample: as many x-planes per component as fit the budget (at least one)
+    planes = max(1, min(n, int(budget_s * 0.7 / (per_pt * 3 * n * n))))
+    t_sl = 0.0
+    pts_done = 0
+    for c in "uvw":
+        npl = planes * n * nzi[c]
+        t0 = time.perf_counter()
+        adv.advect_comp(c, fb[c], mid, 2 * DT, 0, npl)  # far foot (depth 2 dt)
+        adv.advect_comp(c, fb[c], mid, DT, 0, npl)      # near foot
+        t_sl += time.perf_counter() - t0
+        pts_done += npl
+    t_sl_full = t_sl * total_pts / pts_done
+    # z-solve (PCR, as the reference) on the same fraction of columns
+    ncol = max(1, planes * n)
+    t0 = time.perf_counter()
+    a, b, cc = O.zsolve_coefficients("u", (2.0 / 3.0) * DT, n, dz_c, dz_f, 1.0 / RE_B)
+    d = ch.u[1 : 1 + planes, 1 : n + 1, 1 : n + 1].reshape(ncol, n)
+    for _ in range(3):
+        O.pcr_solve(a, b, cc, d)
+    t_z = (time.perf_counter() - t0) * (n * n) / ncol
+    # divergence + FFT Poisson + projection + bulk shift at full size
+    t0 = time.perf_counter()
+    div = ch.divergence()
+    phi = O.solve_poisson_fft(div / ((2.0 / 3.0) * DT), ch.fft)
+    O.project_velocity(ch.u, ch.v, ch.w, phi, n, n, n, ch.dx, ch.dy, ch.dz_c, ch.dz_f, (2.0 / 3.0) * DT)
+    ch.bulk_velocity()
+    t_p = time.perf_counter() - t0
+    t_step = t_sl_full + t_z + t_p
+    desc = (f"oracle (C trace+gather on {threads} threads, numpy rest): trace+gather of both feet on "
+            f"{planes} of {n} x-planes per component ({pts_done} of {total_pts} arrival points) "
+            f"scaled x{total_pts / pts_done:.1f}; PCR z-solve on {ncol} of {n * n} columns scaled; "
+            f"divergence + FFT Poisson + projection + bulk at full size once "
+            f"(trace+gather {t_sl_full:.1f} s, z-solve {t_z:.2f} s, projection {t_p:.2f} s per step)")
+    return t_step, desc, threads
+
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    n, order = args.n, args.order
+    import oracle.slbdf2 as O
+
+    z_f, z_c, dz_f, dz_c = O.generate_grid(GAMMA, n, LZ)
+    u, v, w = initial_field(n, z_f, z_c, 0)
+    ch = O.OracleChannel(n, n, n, LX, LY, LZ, GAMMA, 1.0 / RE_B, u, v, w, order=order, z_f=z_f, z_c=z_c)
+    adv = ch.sl
+    fb = {c: adv.fill(c, f) for c, f in zip("uvw", (ch.u, ch.v, ch.w))}
+    threads = O.max_threads()
+    nzi = {"u": n, "v": n, "w": n - 1}
+    total_pts = sum(n * n * nzi[c] for c in "uvw")
+    # the rest of the step (divergence, FFT Poisson, projection, PCR z-solve) at full size, once
+    t0 = time.perf_counter()
+    div = ch.divergence()
+    phi = O.solve_poisson_fft(div / ((2.0 / 3.0) * DT), ch.fft)
+    O.project_velocity(ch.u, ch.v, ch.w, phi, n, n, n, ch.dx, ch.dy, ch.dz_c, ch.dz_f, (2.0 / 3.0) * DT)
+    t_rest = time.perf_counter() - t0
+    a, b, cc = O.zsolve_coefficients("u", (2.0 / 3.0) * DT, n, dz_c, dz_f, 1.0 / RE_B)
+    t0 = time.perf_counter()
+    O.pcr_solve(a, b, cc, ch.u[1:2, 1 : n + 1, 1 : n + 1].reshape(n, n))
+    t_rest += 3 * (time.perf_counter() - t0) * n
+    # per timed step: trace+gather of both feet for one strip of arrival points per
+    # component, sized so the whole run stays within a few minutes
+    total_steps = args.warmup + args.steps
+    budget_per_step = max(0.05, 150.0 / max(total_steps, 1))
+    probe = n * 16
+    t0 = time.perf_counter()
+    adv.advect_comp("u", fb["u"], fb, 2 * DT, 0, probe)
+    adv.advect_comp("u", fb["u"], fb, DT, 0, probe)
+    per_pt = (time.perf_counter() - t0) / probe
+    strip = max(32, min(n * n, int(budget_per_step / (3 * per_pt))))
+    times = []
+    for it in range(total_steps):
+        t0 = time.perf_counter()
+        for c in "uvw":
+            adv.advect_comp(c, fb[c], fb, 2 * DT, 0, strip)
+            adv.advect_comp(c, fb[c], fb, DT, 0, strip)
+        dt_s = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt_s * total_pts / (3 * strip) + t_rest)
+    t_step = float(np.mean(times))
+    value = 1.0 / t_step
+    sample = (f"oracle port (the CPU restatement of the reference's float64 path; C trace+gather on "
+              f"{threads} threads, numpy rest): per step, trace+gather of both feet for {strip} "
+              f"arrival points per component scaled to all {total_pts}, plus divergence + FFT "
+              f"Poisson + projection + PCR z-solve timed once at full size ({t_rest:.2f} s)")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": f"SL-BDF2 step {n}^3 (4pi x 2pi x 2), Re_b {RE_B}, dt {DT}, "
+                               f"order {order}, FP64", "grid": [n, n, n], "order": order},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_b200(args):
+    import torch
+
+    from slchannel_b200 import _native as N
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = dist_init(world, "nccl")
+    n, order, K, W = args.n, args.order, args.steps, max(args.warmup, 3)
+    flow = build_flow(n, order)
+    dev = torch.cuda.current_device()
+    for _ in range(W):
+        flow.step_sl_bdf2(DT)
+    torch.cuda.synchronize()
+
+    flow._grid.timing(True)
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(gpu_smi_id(dev))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = N.kernel_launches()
+    sampler.start()
+    ev0.record(stream)
+    for _ in range(K):
+        flow.step_sl_bdf2(DT)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = N.kernel_launches() - launches0
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    phases = flow._grid.timing_read()
+    flow._grid.timing(False)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * K / (ms_max / 1000.0)
+
+    # correctness riders for the timed state
+    from slchannel_b200.utils import compute_divergence
+
+    div = compute_divergence(flow.u, flow.v, flow.w, n, n, n, flow.dx, flow.dy, flow.dz_f)
+    max_div = float(div.abs().max())
+
+    # roofline of the dominant kernel (fused trace + gather + BDF2 epilogue)
+    sl_ms, sl_cnt = phases["sl"]
+    t_sl = sl_ms / 1000.0 / max(sl_cnt, 1)
+    bytes_alg, flops_alg, pts = sl_algorithmic(n, order)
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_alg / t_sl / 1e9
+    tpp = profiled_traffic_per_point()
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "traffic": (tpp * pts) if tpp else None,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+        "kernel": f"k_sl<C,{order},BDF2> x3 launches per step (one per velocity component)",
+        "algorithmic_bytes_per_step": bytes_alg,
+        "kernel_ms_per_step": t_sl * 1000.0,
+        "fp64_gflops": flops_alg / t_sl / 1e9,
+        "note": "the FP64 gather is bound by L1/LSU load throughput and the FP64 pipe, not HBM",
+    }
+    phase_ms = {p: (v[0] / max(v[1], 1)) for p, v in phases.items() if v[1]}
+
+    # e2e: the public API (SLChannelFlow.step_sl_bdf2) with the state in pinned
+    # HOST memory: every step uploads V^n, V^{n-1} and downloads V^{n+1}, p, u_bulk
+    Ke = max(1, min(args.e2e_steps, K))
+    host_in = [torch.empty_like(t, device="cpu").pin_memory() for t in
+               (flow.u, flow.v, flow.w, flow.u_nm1, flow.v_nm1, flow.w_nm1)]
+    host_out = [torch.empty_like(t, device="cpu").pin_memory() for t in (flow.u, flow.v, flow.w, flow.p)]
+    host_ub = torch.empty((), dtype=torch.float64).pin_memory()
+    for h, d in zip(host_in, (flow.u, flow.v, flow.w, flow.u_nm1, flow.v_nm1, flow.w_nm1)):
+        h.copy_(d)
+    torch.cuda.synchronize()
+    h2d = sum(t.numel() * 8 for t in host_in)
+    d2h = sum(t.numel() * 8 for t in host_out) + 8
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(Ke):
+        for h, name in zip(host_in, ("u", "v", "w", "u_nm1", "v_nm1", "w_nm1")):
+            getattr(flow, name).copy_(h, non_blocking=True)
+        ub, _f = flow.step_sl_bdf2(DT)
+        for h, name in zip(host_out, ("u", "v", "w", "p")):
+            h.copy_(getattr(flow, name), non_blocking=True)
+        host_ub.copy_(ub, non_blocking=True)
+        # host state rotates: V^{n-1} <- V^n, V^n <- V^{n+1}; the freed V^{n-1}
+        # buffers receive the next download (all copies are ordered on one stream)
+        host_in, host_out = host_out[0:3] + host_in[0:3], host_in[3:6] + host_out[3:4]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_max = e2e_ms
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_max = float(t.item())
+    e2e = {"value": world * Ke / (e2e_max / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "steps": Ke, "ms_per_step": e2e_max / Ke,
+           "path": "SLChannelFlow.step_sl_bdf2 with state in pinned host memory"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"SL-BDF2 step {n}^3 (4pi x 2pi x 2), Re_b {RE_B}, dt {DT}, "
+                               f"order {order}, FP64 (plain drop-in form)",
+                   "grid": [n, n, n], "order": order, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state ~1.8 GB at 256^3)"},
+        "mpoint_updates_per_s": value * 3 * n**3 / 1e6,
+        "phase_ms": phase_ms, "max_div": max_div,
+        "gpu_launches": int(launches), "roofline": roofline, "clocks": clocks, "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_cpu, desc, threads = cpu_step_sample(n, order, args.cpu_budget_s)
+        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

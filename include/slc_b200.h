@@ -1,0 +1,223 @@
+/*
+ * slc_b200.h -- C ABI of the B200 (sm_100a) SL-BDF2 channel step.
+ *
+ * This is the drop-in boundary for slChannel's semi-Lagrangian BDF2 path
+ * (gmcavallazzi/SLchannel v1.0.1; reference paths below are relative to that
+ * project).  A host binding (the Python package slchannel_b200 uses ctypes)
+ * passes plain device pointers, sizes and a cudaStream_t; no torch types cross
+ * this boundary.
+ *
+ * Conventions
+ *  - Fields are float64, row-major (x, y, z) with z contiguous, in the
+ *    reference's ghost-shaped layouts (one ghost layer per side):
+ *      u (nx+1, ny+2, nz+2)   v (nx+2, ny+1, nz+2)   w (nx+2, ny+2, nz+1)
+ *      p (nx+2, ny+2, nz+2)
+ *    The caller owns field memory; the library owns its tables, FFT plans and
+ *    workspaces (allocated in slc_grid_create).
+ *  - Every function returns 0 on success or a nonzero SLC_E* code; it never
+ *    traps.  slc_last_error() gives the message of the last failure on that
+ *    handle.  Work is enqueued on `stream` (NULL = legacy default stream) and
+ *    is asynchronous unless stated otherwise.
+ *  - A handle is not thread-safe: use one handle per host thread / stream.
+ */
+#ifndef SLC_B200_H
+#define SLC_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SLC_API __attribute__((visibility("default")))
+#else
+#define SLC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLC_OK 0
+#define SLC_E_INVALID 1 /* bad argument (maps to the reference's ValueError) */
+#define SLC_E_CUDA 2    /* a CUDA runtime / driver call failed (RuntimeError) */
+#define SLC_E_CUFFT 3   /* a cuFFT call failed (RuntimeError) */
+#define SLC_E_NOMEM 4   /* device allocation failed (RuntimeError) */
+
+#define SLC_PREC_FP64 0  /* plain float64 path (parity form) */
+#define SLC_PREC_MIXED 1 /* FP32 fluctuation about an FP64 plane mean in trace+gather */
+
+typedef struct slc_grid slc_grid; /* opaque */
+
+/* Grid description.  Mirrors the arguments of
+ * SLAdvector.__init__ (slchannel/semilag.py:133-153) plus the transport
+ * and boundary parameters the step needs (slchannel/solver.py:168-282). */
+typedef struct {
+    int32_t nx, ny, nz;        /* interior cells; x, y periodic, z walls */
+    double Lx, Ly, Lz;         /* domain extents */
+    double gamma;              /* tanh stretching parameter */
+    int32_t stretching;        /* 0 = 'symmetric', 1 = 'bottom' */
+    int32_t order;             /* 4 (tricubic) or 6 (triquintic) */
+    int32_t traj_order;        /* 2 (trilinear); 4 is not implemented here */
+    int32_t n_traj_iters;      /* midpoint fixed-point iterations (>= 1) */
+    int32_t top_wall_neumann;  /* 0 = 'dirichlet' (no-slip), 1 = 'neumann' */
+    int32_t precision;         /* SLC_PREC_FP64 or SLC_PREC_MIXED */
+    double nu;                 /* kinematic viscosity 1/Re */
+    const double *z_f;         /* HOST pointer, nz+1 face coordinates */
+    const double *z_c;         /* HOST pointer, nz+2 centres incl. ghosts */
+    int32_t device;            /* CUDA device ordinal the handle lives on */
+    int32_t xy_rhs_lagged;     /* 0 = 'extrap' (2R^n - R^{n-1}), 1 = 'lagged' (R^n) */
+} slc_grid_desc;
+
+/* Library version string, e.g. "slc_b200 0.1". */
+SLC_API const char *slc_version(void);
+
+/* Build a handle: z tables, Lagrange inverse-denominator tables, cuFFT plans
+ * and workspaces.  Replaces SLAdvector.__init__ (semilag.py:133-381) and
+ * initialize_fft_solver (slchannel/projection.py:24-131).  Synchronous. */
+SLC_API int slc_grid_create(const slc_grid_desc *desc, slc_grid **out);
+
+/* Release a handle and everything it allocated.  Synchronous. */
+SLC_API int slc_grid_destroy(slc_grid *g);
+
+/* Message of the last failure on `g` (or of the last failed create when
+ * g == NULL).  Valid until the next call on the handle. */
+SLC_API const char *slc_last_error(const slc_grid *g);
+
+/* Ghost-cell boundary conditions on u, v, w in place: periodic x, y; no-slip
+ * (or free-slip top) u, v; w = 0 on both walls.
+ * Replaces apply_bc_all (slchannel/solver.py:70-107). */
+SLC_API int slc_apply_bc(slc_grid *g, double *u, double *v, double *w, void *stream);
+
+/* Continuous face index of n wall-normal coordinates (device arrays).
+ * Replaces SLAdvector._face_coord (semilag.py:400-411). */
+SLC_API int slc_face_coord(slc_grid *g, const double *z, int64_t n, double *kf, void *stream);
+
+/* Interpolate one component's node buffer (NX, NY, NZ) contiguous, at n
+ * arbitrary points with Lagrange order 2, 4 or 6.  With count_clamp, z is
+ * clamped to [z_lo, z_hi] and the clamps are ADDED to *nclamp (device int64).
+ * Replaces SLAdvector._build_iw + _apply_iw (semilag.py:460-510). */
+SLC_API int slc_interp_points(slc_grid *g, int comp, int order, const double *nodebuf, const double *x,
+                      const double *y, const double *z, int64_t n, int count_clamp, double *out,
+                      int64_t *nclamp, void *stream);
+
+/* Departure points (x_d, y_d, z_d) of every arrival point of `comp`
+ * (arrival-shaped, z fastest), traced through the trajectory velocity given
+ * as three node buffers (NX, NY, NZ) contiguous.
+ * Replaces SLAdvector.departure_coords (semilag.py:534-552). */
+SLC_API int slc_departure(slc_grid *g, int comp, const double *mid_u, const double *mid_v,
+                  const double *mid_w, double dt, double *xd, double *yd, double *zd,
+                  void *stream);
+
+/* One semi-Lagrangian foot for all three components: trace each arrival
+ * point through (mid_u, mid_v, mid_w) over dt and interpolate (fu, fv, fw)
+ * there.  All inputs and outputs are ghost-shaped; only the interiors of
+ * ou, ov, ow are written (w wall faces and ghosts untouched).  The number of
+ * clamped feet is WRITTEN to *nclamp (device int64).
+ * Replaces SLAdvector.advect (semilag.py:584-671). */
+SLC_API int slc_advect(slc_grid *g, const double *fu, const double *fv, const double *fw,
+               const double *mid_u, const double *mid_v, const double *mid_w, double dt,
+               double *ou, double *ov, double *ow, int64_t *nclamp, void *stream);
+
+/* Fused BDF2 predictor: both feet of every arrival point traced with
+ * U* = 2 V^n - V^{n-1} (depths dt and 2 dt), V^n and V^{n-1} interpolated
+ * there, and u_hat = 4/3 ubar - 1/3 ubarbar + (2/3) dt (2 R^n - R^{n-1})
+ * written to the interiors of (ou, ov, ow), R the explicit x,y diffusion.
+ * cur/prev/out are ghost-shaped; cur and prev must be BC-consistent.
+ * *nclamp (device int64) receives the clamp count over both feet.
+ * Replaces solver.py:846-903 (the two SLAdvector.advect calls and the
+ * BDF2 combination). */
+SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *vn, const double *wn,
+                          const double *unm1, const double *vnm1, const double *wnm1, double dt,
+                          double *ou, double *ov, double *ow, int64_t *nclamp, void *stream);
+
+/* theta = 1 implicit wall-normal diffusion, in place on the interiors:
+ * (I - dt nu Dzz) f_new = f.
+ * Replaces solve_implicit_diffusion_{u,v,w} (slchannel/operators.py:382-630). */
+SLC_API int slc_zsolve(slc_grid *g, double *u, double *v, double *w, double dt, void *stream);
+
+/* Divergence of the staggered field, interior-shaped (nx, ny, nz) output.
+ * Replaces compute_divergence (slchannel/utils.py:166-180). */
+SLC_API int slc_divergence(slc_grid *g, const double *u, const double *v, const double *w, double *div,
+                   void *stream);
+
+/* Handle-free divergence for callers that hold only the grid spacings:
+ * dz_f is a device array of nz face spacings.  Same result as slc_divergence.
+ * Replaces compute_divergence (slchannel/utils.py:166-180) as called with
+ * explicit (nx, ny, nz, dx, dy, dz_f). */
+SLC_API int slc_divergence_raw(int nx, int ny, int nz, double dx, double dy, const double *dz_f,
+                               const double *u, const double *v, const double *w, double *div,
+                               void *stream);
+
+/* Pressure projection: phi solves Lap phi = div(u)/dt_div (FFT in x, y,
+ * Thomas in z, (0,0) mode pinned); u -= dt_proj grad phi on the interiors;
+ * p (ghost-shaped) receives phi with its ghost cells; then BCs on u, v, w.
+ * Replaces compute_divergence + solve_poisson_fft + project_velocity
+ * (slchannel/projection.py:133-272, solver.py:983-998). */
+SLC_API int slc_project(slc_grid *g, double *u, double *v, double *w, double *p, double dt_div,
+                double dt_proj, void *stream);
+
+/* Bulk velocity sum(u dx dy dz_f) / (Lx Ly Lz) into *out (device double).
+ * Replaces compute_bulk_velocity (slchannel/utils.py:147-163). */
+SLC_API int slc_bulk_velocity(slc_grid *g, const double *u, double *out, void *stream);
+
+/* Number of doubles of device scratch slc_bulk_velocity_raw needs. */
+SLC_API int slc_bulk_scratch_doubles(void);
+
+/* Handle-free bulk velocity: out = inv_volume * sum_{i,j,k} u_int(i,j,k) *
+ * vol_k[k], with vol_k the per-level cell volume dx*dy*dz_f (device, nz) and
+ * scratch at least slc_bulk_scratch_doubles() device doubles.  Summed in a
+ * fixed order (bit-reproducible).
+ * Replaces compute_bulk_velocity (slchannel/utils.py:147-163) for the
+ * cell-volume tensor the solver builds (solver.py:303-306). */
+SLC_API int slc_bulk_velocity_raw(int nx, int ny, int nz, const double *u, const double *vol_k,
+                                  double inv_volume, double *scratch, double *out, void *stream);
+
+/* Exact mass-flux constraint: c = U_bulk - bulk(u); u_int += c; BCs;
+ * out2[0] = bulk(u) after the shift, out2[1] = c / dt (device doubles).
+ * Replaces SLChannelFlow._apply_bulk_forcing (slchannel/solver.py:694-723). */
+SLC_API int slc_bulk_shift(slc_grid *g, double *u, double *v, double *w, double U_bulk, double dt,
+                   double *out2, void *stream);
+
+/* One BDF1 bootstrap step up to (not including) the bulk shift:
+ * next <- advect(cur; U* = cur, dt) + dt R(cur); z-solve at dt; projection
+ * at dt; p <- phi.  cur gets its BCs applied first.  The caller afterwards
+ * treats cur as V^{n-1} and next as V^n.
+ * Replaces SLChannelFlow._step_sl_bdf1_bootstrap (solver.py:729-811)
+ * without its final _bdf2_forcing_update call. */
+SLC_API int slc_step_bdf1(slc_grid *g, double *const cur[3], double *const next[3], double *p, double dt,
+                  int64_t *nclamp, void *stream);
+
+/* One BDF2 step up to (not including) the bulk shift: slc_trace_gather_bdf2
+ * into next, z-solve at 2dt/3, projection at 2dt/3, p <- phi.  The caller
+ * afterwards rotates (prev, cur, next) <- (cur, next, prev).
+ * Replaces SLChannelFlow.step_sl_bdf2 (solver.py:813-1018, noninc pressure)
+ * without its final _bdf2_forcing_update call. */
+SLC_API int slc_step_bdf2(slc_grid *g, double *const cur[3], double *const prev[3], double *const next[3],
+                  double *p, double dt, int64_t *nclamp, void *stream);
+
+/* ---- Profiling -------------------------------------------------------------
+ * Phases timed with CUDA events on the launching stream when timing is on. */
+#define SLC_PHASE_BC 0      /* start-of-step boundary conditions */
+#define SLC_PHASE_MID 1     /* U* = 2 V^n - V^{n-1} */
+#define SLC_PHASE_SL 2      /* fused trace + gather (+ BDF epilogue) kernels */
+#define SLC_PHASE_ZSOLVE 3  /* implicit wall-normal diffusion */
+#define SLC_PHASE_PROJECT 4 /* divergence, FFTs, Thomas, projection, BCs */
+#define SLC_PHASE_BULK 5    /* bulk-flux shift */
+#define SLC_NPHASE 6
+
+/* Turn per-phase event timing on (1) or off (0) for a handle; resets the
+ * accumulated record.  Adds two cudaEventRecord calls per phase per call. */
+SLC_API int slc_timing(slc_grid *g, int enable);
+
+/* Synchronise on the recorded events and return, per phase, the summed
+ * elapsed milliseconds and the number of timed intervals; resets the record.
+ * ms and count each hold SLC_NPHASE entries. */
+SLC_API int slc_timing_read(slc_grid *g, double *ms, int64_t *count);
+
+/* Number of kernels this library has launched in the process so far (its
+ * own kernels; cuFFT's are not counted). */
+SLC_API int64_t slc_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLC_B200_H */

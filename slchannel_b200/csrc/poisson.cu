@@ -1,0 +1,423 @@
+// poisson.cu -- ghost-cell boundary conditions, divergence, the FFT-Poisson
+// tridiagonal sweep, the projection and the bulk-flux reductions (sm_100a).
+//
+// Layout of the Poisson workspaces: the right-hand side and phi are z-major
+// planes rhs[k][i][j] (j fastest), so cuFFT transforms nz contiguous (nx, ny)
+// planes and every (kx, ky) column of the half spectrum hat[k][kx][ky] is
+// walked by one thread with coalesced accesses across the warp.  The
+// divergence and projection kernels transpose between that layout and the
+// z-contiguous velocity arrays through a 32 x 32 shared-memory tile.
+#include "slc_internal.h"
+
+namespace {
+
+// --------------------------------------------------------------------------
+// Boundary conditions (solver.py:70-107; projection.py:180-195 for p).
+// Every ghost element is a copy (or a negated copy) of one interior element,
+// so each is gathered independently from its source.
+// --------------------------------------------------------------------------
+
+struct BcCounts {
+    long long a, b, c;  // x-ghost planes, y-ghost planes (x interior), z-ghost planes
+};
+
+__device__ __host__ inline int n_xghost(int C) { return C == 0 ? 1 : 2; }
+__device__ __host__ inline int n_yghost(int C) { return C == 1 ? 1 : 2; }
+
+__host__ __device__ inline BcCounts bc_counts(int C, int nx, int ny, int nz)
+{
+    GhostShape g = ghost_shape(C, nx, ny, nz);
+    BcCounts r;
+    r.a = (long long)n_xghost(C) * g.Y * g.Z;
+    r.b = (long long)nx * n_yghost(C) * g.Z;
+    r.c = (long long)nx * ny * 2;
+    return r;
+}
+
+__device__ inline void bc_one(const SlcParams &P, int C, double *f, long long t)
+{
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const GhostShape g = ghost_shape(C, nx, ny, nz);
+    const BcCounts cnt = bc_counts(C, nx, ny, nz);
+    int I, J, K;
+    if (t < cnt.a) {
+        K = (int)(t % g.Z);
+        long long q = t / g.Z;
+        J = (int)(q % g.Y);
+        const int which = (int)(q / g.Y);
+        I = which == 0 ? 0 : nx + 1;
+    } else if (t < cnt.a + cnt.b) {
+        t -= cnt.a;
+        K = (int)(t % g.Z);
+        long long q = t / g.Z;
+        const int which = (int)(q % n_yghost(C));
+        I = (int)(q / n_yghost(C)) + 1;
+        J = which == 0 ? 0 : ny + 1;
+    } else {
+        t -= cnt.a + cnt.b;
+        const int which = (int)(t & 1);
+        long long q = t >> 1;
+        J = (int)(q % ny) + 1;
+        I = (int)(q / ny) + 1;
+        K = which == 0 ? 0 : g.Z - 1;
+    }
+    // periodic sources in x and y
+    int Is = I, Js = J;
+    if (C == 0) {
+        if (I == 0) Is = nx;
+    } else {
+        if (I == 0) Is = nx;
+        else if (I == nx + 1) Is = 1;
+    }
+    if (C == 1) {
+        if (J == 0) Js = ny;
+    } else {
+        if (J == 0) Js = ny;
+        else if (J == ny + 1) Js = 1;
+    }
+    double val;
+    if (C == 2) {
+        if (K == 0 || K == nz) val = 0.0;  // impermeable walls
+        else val = f[(size_t)Is * g.Y * g.Z + (size_t)Js * g.Z + K];
+    } else if (C == 3) {  // pressure: Neumann copies in z
+        int Ks = K == 0 ? 1 : (K == nz + 1 ? nz : K);
+        val = f[(size_t)Is * g.Y * g.Z + (size_t)Js * g.Z + Ks];
+    } else {
+        double sign = 1.0;
+        int Ks = K;
+        if (K == 0) {
+            Ks = 1;
+            sign = -1.0;
+        } else if (K == nz + 1) {
+            Ks = nz;
+            sign = P.top_neumann ? 1.0 : -1.0;
+        }
+        val = sign * f[(size_t)Is * g.Y * g.Z + (size_t)Js * g.Z + Ks];
+    }
+    f[(size_t)I * g.Y * g.Z + (size_t)J * g.Z + K] = val;
+}
+
+__global__ void k_apply_bc(SlcParams P, double *u, double *v, double *w, double *p, long long n0,
+                           long long n1, long long n2, long long n3)
+{
+    const long long total = n0 + n1 + n2 + n3;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t < n0) bc_one(P, 0, u, t);
+        else if (t < n0 + n1) bc_one(P, 1, v, t - n0);
+        else if (t < n0 + n1 + n2) bc_one(P, 2, w, t - n0 - n1);
+        else bc_one(P, 3, p, t - n0 - n1 - n2);
+    }
+}
+
+// --------------------------------------------------------------------------
+// Divergence (utils.py:166-180).  The x-1 / y-1 neighbours use the periodic
+// image directly, so the field's ghosts need not be current.
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ double div_at(const SlcParams &P, const double *__restrict__ u,
+                                         const double *__restrict__ v,
+                                         const double *__restrict__ w,
+                                         const double *__restrict__ dz_f, int i, int j, int k)
+{
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const size_t usx = (size_t)(ny + 2) * (nz + 2), usy = nz + 2;
+    const size_t vsx = (size_t)(ny + 1) * (nz + 2), vsy = nz + 2;
+    const size_t wsx = (size_t)(ny + 2) * (nz + 1), wsy = nz + 1;
+    const int im = i == 0 ? nx : i;  // u row i (0-based interior i-1) ; ghost row 0 == row nx
+    const int jm = j == 0 ? ny : j;
+    const double du = (u[(i + 1) * usx + (j + 1) * usy + k + 1] - u[im * usx + (j + 1) * usy + k + 1]) / P.dx;
+    const double dv = (v[(i + 1) * vsx + (j + 1) * vsy + k + 1] - v[(i + 1) * vsx + jm * vsy + k + 1]) / P.dy;
+    const double dw = (w[(i + 1) * wsx + (j + 1) * wsy + k + 1] - w[(i + 1) * wsx + (j + 1) * wsy + k]) / dz_f[k];
+    return du + dv + dw;
+}
+
+// rhs[k][i][j] = div(i, j, k) / dt_div, through a shared-memory transpose.
+__global__ void __launch_bounds__(256) k_div_pack(SlcParams P, const double *__restrict__ u,
+                                                  const double *__restrict__ v,
+                                                  const double *__restrict__ w,
+                                                  const double *__restrict__ dz_f, double dt_div,
+                                                  double *__restrict__ rhs)
+{
+    __shared__ double tile[32][33];
+    const int i = blockIdx.z, j0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const int j = j0 + r, k = k0 + tx;
+        double val = 0.0;
+        if (j < P.ny && k < P.nz) val = div_at(P, u, v, w, dz_f, i, j, k) / dt_div;
+        tile[r][tx] = val;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int k = k0 + r, j = j0 + tx;
+        if (k < P.nz && j < P.ny) rhs[((size_t)k * P.nx + i) * P.ny + j] = tile[tx][r];
+    }
+}
+
+__global__ void k_divergence(SlcParams P, const double *__restrict__ u,
+                             const double *__restrict__ v, const double *__restrict__ w,
+                             const double *__restrict__ dz_f, double *__restrict__ div)
+{
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % P.nz);
+        const long long q = t / P.nz;
+        const int j = (int)(q % P.ny), i = (int)(q / P.ny);
+        div[t] = div_at(P, u, v, w, dz_f, i, j, k);
+    }
+}
+
+// --------------------------------------------------------------------------
+// Thomas sweep per (kx, ky) column of the half spectrum (projection.py:199-247)
+// with the modified-wavenumber diagonals (projection.py:47-114) built on the
+// fly; the (0, 0) mode's first row is the identity (projection.py:113-114).
+// The inverse-FFT normalisation 1/(nx ny) is folded into the back
+// substitution.
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_thomas(SlcParams P, double2 *__restrict__ hat,
+                                                double *__restrict__ cpw,
+                                                const double *__restrict__ kx2,
+                                                const double *__restrict__ ky2,
+                                                const double *__restrict__ cl,
+                                                const double *__restrict__ cr, double norm)
+{
+    const int nky = P.ny / 2 + 1;
+    const long long ncol = (long long)P.nx * nky;
+    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int nz = P.nz;
+    const int kx = (int)(col / nky), ky = (int)(col % nky);
+    const double k2 = kx2[kx] + ky2[ky];
+    const size_t st = (size_t)ncol;
+
+    double b = -(cl[0] + cr[0] + k2) + cl[0];
+    if (nz == 1) b += cr[0];
+    double c = nz > 1 ? cr[0] : 0.0;
+    if (col == 0) {
+        b = 1.0;
+        c = 0.0;
+    }
+    double id = 1.0 / b;
+    double cprev = c * id;
+    double2 d = hat[col];
+    double2 dp = make_double2(d.x * id, d.y * id);
+    hat[col] = dp;
+    cpw[col] = cprev;
+    for (int k = 1; k < nz; ++k) {
+        const double a = cl[k];
+        double bk = -(cl[k] + cr[k] + k2);
+        if (k == nz - 1) bk += cr[nz - 1];
+        const double ck = (k < nz - 1) ? cr[k] : 0.0;
+        const double denom = bk - a * cprev;
+        id = 1.0 / denom;
+        cprev = ck * id;
+        d = hat[k * st + col];
+        dp = make_double2((d.x - a * dp.x) * id, (d.y - a * dp.y) * id);
+        hat[k * st + col] = dp;
+        cpw[k * st + col] = cprev;
+    }
+    double2 x = dp;
+    hat[(size_t)(nz - 1) * st + col] = make_double2(x.x * norm, x.y * norm);
+    for (int k = nz - 2; k >= 0; --k) {
+        const double2 dk = hat[k * st + col];
+        const double ck = cpw[k * st + col];
+        x = make_double2(dk.x - ck * x.x, dk.y - ck * x.y);
+        hat[k * st + col] = make_double2(x.x * norm, x.y * norm);
+    }
+}
+
+// --------------------------------------------------------------------------
+// Projection (projection.py:250-272): u -= dt dphi/dx, v -= dt dphi/dy,
+// w -= dt dphi/dz on the interiors, p interior <- phi.  phi is z-major; a tile
+// (i fixed, 33 j x 33 k, plus the x+1 plane) goes through shared memory.
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_project(SlcParams P, const double *__restrict__ phi,
+                                                 double *__restrict__ u, double *__restrict__ v,
+                                                 double *__restrict__ w, double *__restrict__ p,
+                                                 const double *__restrict__ dz_c, double dt)
+{
+    __shared__ double t0[33][33];  // [k][j], plane i
+    __shared__ double t1[32][33];  // [k][j], plane i+1 (periodic)
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int i = blockIdx.z, j0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int i1 = (i + 1 == nx) ? 0 : i + 1;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 33; r += 8) {
+        const int k = k0 + r;
+        if (k >= nz) continue;
+        for (int c = tx; c < 33; c += 32) {
+            int j = j0 + c;
+            if (j > ny) continue;
+            if (j == ny) j = 0;
+            t0[r][c] = phi[((size_t)k * nx + i) * ny + j];
+            if (r < 32 && c < 32) t1[r][c] = phi[((size_t)k * nx + i1) * ny + j];
+        }
+    }
+    __syncthreads();
+    const size_t usx = (size_t)(ny + 2) * (nz + 2), usy = nz + 2;
+    const size_t vsx = (size_t)(ny + 1) * (nz + 2), vsy = nz + 2;
+    const size_t wsx = (size_t)(ny + 2) * (nz + 1), wsy = nz + 1;
+    const size_t psx = (size_t)(ny + 2) * (nz + 2), psy = nz + 2;
+    for (int r = ty; r < 32; r += 8) {
+        const int j = j0 + r, k = k0 + tx;
+        if (j >= ny || k >= nz) continue;
+        const double f0 = t0[tx][r];
+        const double fx = t1[tx][r];
+        const double fy = t0[tx][r + 1];
+        const size_t I = i + 1, J = j + 1, K = k + 1;
+        u[I * usx + J * usy + K] -= dt * ((fx - f0) / P.dx);
+        v[I * vsx + J * vsy + K] -= dt * ((fy - f0) / P.dy);
+        if (k < nz - 1) {
+            const double fz = t0[tx + 1][r];
+            w[I * wsx + J * wsy + K] -= dt * ((fz - f0) / dz_c[k + 1]);
+        }
+        p[I * psx + J * psy + K] = f0;
+    }
+}
+
+// --------------------------------------------------------------------------
+// Bulk velocity (utils.py:147-163): sum u dx dy dz_f / (Lx Ly Lz), summed in a
+// fixed order (fixed grid, fixed block tree, fixed finish) so reruns agree
+// bit for bit.  With c_dev, the shift u += c (solver.py:714-717) is applied
+// first and the sum taken over the shifted field.
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_bulk_partials(SlcParams P, double *__restrict__ u,
+                                                       const double *__restrict__ dz_f,
+                                                       const double *__restrict__ c_dev,
+                                                       double *__restrict__ partials)
+{
+    __shared__ double red[256];
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long n = (long long)nx * ny * nz;
+    const double c = c_dev ? *c_dev : 0.0;
+    const size_t usx = (size_t)(ny + 2) * (nz + 2), usy = nz + 2;
+    double acc = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % nz);
+        const long long q = t / nz;
+        const int j = (int)(q % ny), i = (int)(q / ny);
+        double *up = u + (size_t)(i + 1) * usx + (size_t)(j + 1) * usy + (k + 1);
+        double val = *up;
+        if (c_dev) {
+            val = val + c;
+            *up = val;
+        }
+        acc = fma(val, dz_f[k], acc);
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+}
+
+__global__ void k_bulk_finish(const double *__restrict__ partials, int nparts, double dxdy_over_V,
+                              double U_bulk, double dt, double *bulk_out, double *shift_out)
+{
+    __shared__ double red[256];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) acc += partials[b];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double bulk = red[0] * dxdy_over_V;
+        if (bulk_out) *bulk_out = bulk;
+        if (shift_out) {
+            const double corr = U_bulk - bulk;
+            shift_out[0] = corr;
+            shift_out[1] = corr / dt;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_apply_bc(const SlcParams &P, double *u, double *v, double *w, double *p,
+                            cudaStream_t s)
+{
+    auto tot = [&](int C) {
+        BcCounts c = bc_counts(C, P.nx, P.ny, P.nz);
+        return c.a + c.b + c.c;
+    };
+    const long long n0 = u ? tot(0) : 0, n1 = v ? tot(1) : 0, n2 = w ? tot(2) : 0,
+                    n3 = p ? tot(3) : 0;
+    const long long total = n0 + n1 + n2 + n3;
+    if (total == 0) return cudaSuccess;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_apply_bc<<<(unsigned)blocks, 256, 0, s>>>(P, u, v, w, p, n0, n1, n2, n3);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_div_pack(const SlcParams &P, Tri f, const double *dz_f, double dt_div,
+                            double *rhs_zmajor, cudaStream_t s)
+{
+    dim3 grid((P.nz + 31) / 32, (P.ny + 31) / 32, P.nx), block(32, 8);
+    k_div_pack<<<grid, block, 0, s>>>(P, f.u, f.v, f.w, dz_f, dt_div, rhs_zmajor);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_divergence(const SlcParams &P, Tri f, const double *dz_f, double *div,
+                              cudaStream_t s)
+{
+    long long n = (long long)P.nx * P.ny * P.nz;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_divergence<<<(unsigned)blocks, 256, 0, s>>>(P, f.u, f.v, f.w, dz_f, div);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_thomas_poisson(const SlcParams &P, double *hat, double *cp, const double *kx2,
+                                  const double *ky2, const double *cl, const double *cr,
+                                  cudaStream_t s)
+{
+    const long long ncol = (long long)P.nx * (P.ny / 2 + 1);
+    const double norm = 1.0 / ((double)P.nx * (double)P.ny);
+    k_thomas<<<(unsigned)((ncol + 255) / 256), 256, 0, s>>>(P, (double2 *)hat, cp, kx2, ky2, cl,
+                                                          cr, norm);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project(const SlcParams &P, const double *phi_zmajor, TriMut f, double *p,
+                           const double *dz_c, double dt, cudaStream_t s)
+{
+    dim3 grid((P.nz + 31) / 32, (P.ny + 31) / 32, P.nx), block(32, 8);
+    k_project<<<grid, block, 0, s>>>(P, phi_zmajor, f.u, f.v, f.w, p, dz_c, dt);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bulk_partials(const SlcParams &P, double *u, const double *dz_f,
+                                 const double *c_dev, double *partials, cudaStream_t s)
+{
+    k_bulk_partials<<<kBulkBlocks, 256, 0, s>>>(P, u, dz_f, c_dev, partials);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bulk_finish(const SlcParams &P, const double *partials, double Lx, double Ly,
+                               double U_bulk, double dt, double *bulk_out, double *shift_out,
+                               cudaStream_t s)
+{
+    const double dxdy_over_V = (P.dx * P.dy) / (Lx * Ly * P.Lz);
+    k_bulk_finish<<<1, 256, 0, s>>>(partials, kBulkBlocks, dxdy_over_V, U_bulk, dt, bulk_out,
+                                    shift_out);
+    count_launches(1);
+    return cudaGetLastError();
+}

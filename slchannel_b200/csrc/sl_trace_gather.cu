@@ -1,0 +1,307 @@
+// sl_trace_gather.cu -- the fused semi-Lagrangian trace + Lagrange gather
+// (+ BDF2 epilogue) for sm_100a.
+//
+// One thread per arrival point.  The midpoint fixed-point iteration
+// (semilag.py:534-552) samples the frozen trajectory velocity trilinearly;
+// its first iteration is evaluated at the arrival point itself and is shared
+// by the near (dt) and the far (2 dt) foot, which are otherwise integrated
+// independently from the arrival point (solver.py:813-826).  Both feet stay in
+// registers; the order-O tensor-product Lagrange interpolation
+// (semilag.py:44-59, 426-500) reads V^n / V^{n-1} directly from the caller's
+// ghost-shaped arrays (periodic wrap by index arithmetic instead of the
+// reference's node-buffer copy, semilag.py:387-394), and the epilogue forms
+// 4/3 ubar - 1/3 ubarbar + dt_eff (2 R^n - R^{n-1}) with the explicit x,y
+// diffusion R evaluated at the arrival point (operators.py:293-367,
+// solver.py:846-903).
+#include "slc_internal.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Vel3 {
+    NodeView<double> u, v, w;
+};
+
+__device__ __forceinline__ void add_clamps(unsigned long long *counter, unsigned cnt)
+{
+    unsigned tot = __reduce_add_sync(0xffffffffu, cnt);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(counter, (unsigned long long)tot);
+}
+
+// Trajectory velocity at one point (semilag.py:512-528, traj_order = 2):
+// z clamped to [z_lo, z_hi], one face-locate shared by the three samples.
+__device__ __forceinline__ void sample3(const SlcParams &P, const Vel3 &M, double x, double y,
+                                        double z, double &us, double &vs, double &ws)
+{
+    double zc = clampz(P, z);
+    int c = face_cell(P, zc);
+    us = trilinear<0>(P, M.u, x, y, zc, c);
+    vs = trilinear<1>(P, M.v, x, y, zc, c);
+    ws = trilinear<2>(P, M.w, x, y, zc, c);
+}
+
+// Iterated midpoint rule continued from the first-iteration sample
+// (us0, vs0, ws0) taken at the arrival point; returns the unclamped foot.
+__device__ __forceinline__ void trace_foot(const SlcParams &P, const Vel3 &M, double xa, double ya,
+                                           double za, double half_dt, double us0, double vs0,
+                                           double ws0, double &xd, double &yd, double &zd)
+{
+    double xm = xa - half_dt * us0;
+    double ym = ya - half_dt * vs0;
+    double zm = clampz(P, za - half_dt * ws0);
+    for (int it = 1; it < P.n_iters; ++it) {
+        double us, vs, ws;
+        sample3(P, M, xm, ym, zm, us, vs, ws);
+        xm = xa - half_dt * us;
+        ym = ya - half_dt * vs;
+        zm = clampz(P, za - half_dt * ws);
+    }
+    xd = 2.0 * xm - xa;
+    yd = 2.0 * ym - ya;
+    zd = 2.0 * zm - za;
+}
+
+// Clamp-and-count the foot (semilag.py:472-474) and interpolate F there.
+template <int C, int O>
+__device__ __forceinline__ double gather_foot(const SlcParams &P, NodeView<double> F, double xd,
+                                              double yd, double zd, unsigned &ncl)
+{
+    if (zd < P.z_lo || zd > P.z_hi) ncl += 1;
+    double z = clampz(P, zd);
+    int c = face_cell(P, z);
+    Stencil<O, double> st;
+    build_stencil<C, O, double>(P, F.sx, F.sy, xd, yd, z, c, st);
+    return gather_sum<O, double, double>(F.p, st);
+}
+
+// nu (d2/dx2 + d2/dy2) f at interior point (i, j, k) of component C, with the
+// reference's periodic extensions u[nx+1] = u[1] and v[:, ny+1] = v[:, 1]
+// (operators.py:301-306, 329-333).
+template <int C>
+__device__ __forceinline__ double xy_diffusion(const SlcParams &P, const double *__restrict__ f,
+                                               int i, int j, int k)
+{
+    GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
+    const size_t sx = (size_t)g.Y * g.Z, sy = g.Z;
+    const int I = i + 1, J = j + 1, K = k + 1;
+    int Ip = I + 1, Jp = J + 1;
+    if (C == 0 && Ip == P.nx + 1) Ip = 1;
+    if (C == 1 && Jp == P.ny + 1) Jp = 1;
+    const double fc = __ldg(f + I * sx + J * sy + K);
+    const double d2x =
+        (__ldg(f + Ip * sx + J * sy + K) - 2.0 * fc + __ldg(f + (I - 1) * sx + J * sy + K)) * P.inv_dx2;
+    const double d2y =
+        (__ldg(f + I * sx + Jp * sy + K) - 2.0 * fc + __ldg(f + I * sx + (J - 1) * sy + K)) * P.inv_dy2;
+    return P.nu * (d2x + d2y);
+}
+
+// MODE 0: one foot of depth dt on field fn (SLAdvector.advect).
+// MODE 1: BDF1 predictor ubar + dt R(fn)            (solver.py:760-771).
+// MODE 2: BDF2 predictor 4/3 ubar - 1/3 ubarbar + (2/3)dt Rh (solver.py:846-903).
+template <int C, int O, int MODE>
+__global__ void __launch_bounds__(kThreads) k_sl(SlcParams P, Vel3 M, const double *__restrict__ fn,
+                                                 const double *__restrict__ fnm1, double dt,
+                                                 double *__restrict__ out,
+                                                 unsigned long long *nclamp)
+{
+    const int nzi = (C == 2) ? P.nz - 1 : P.nz;
+    const long long n = (long long)P.nx * P.ny * nzi;
+    const long long p = (long long)blockIdx.x * kThreads + threadIdx.x;
+    unsigned ncl = 0;
+    if (p < n) {
+        const int k = (int)(p % nzi);
+        const long long q = p / nzi;
+        const int j = (int)(q % P.ny);
+        const int i = (int)(q / P.ny);
+        double xa, ya, za;
+        arrival_point<C>(P, i, j, k, xa, ya, za);
+        double us0, vs0, ws0;
+        sample3(P, M, xa, ya, za, us0, vs0, ws0);
+
+        const NodeView<double> Fn = ghost_view<double>(C, fn, P.nx, P.ny, P.nz);
+        double xd, yd, zd;
+        trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd, yd, zd);
+        const double ubar = gather_foot<C, O>(P, Fn, xd, yd, zd, ncl);
+        double res;
+        if (MODE == 0) {
+            res = ubar;
+        } else if (MODE == 1) {
+            res = ubar + dt * xy_diffusion<C>(P, fn, i, j, k);
+        } else {
+            const NodeView<double> Fm = ghost_view<double>(C, fnm1, P.nx, P.ny, P.nz);
+            trace_foot(P, M, xa, ya, za, dt, us0, vs0, ws0, xd, yd, zd);  // half of 2 dt
+            const double ubb = gather_foot<C, O>(P, Fm, xd, yd, zd, ncl);
+            const double Rn = xy_diffusion<C>(P, fn, i, j, k);
+            const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion<C>(P, fnm1, i, j, k);
+            res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
+            res = res + ((2.0 / 3.0) * dt) * Rh;
+        }
+        const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
+        out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
+    }
+    add_clamps(nclamp, ncl);
+}
+
+template <int C>
+__global__ void __launch_bounds__(kThreads) k_departure(SlcParams P, Vel3 M, double dt,
+                                                        double *xd, double *yd, double *zd)
+{
+    const int nzi = (C == 2) ? P.nz - 1 : P.nz;
+    const long long n = (long long)P.nx * P.ny * nzi;
+    const long long p = (long long)blockIdx.x * kThreads + threadIdx.x;
+    if (p >= n) return;
+    const int k = (int)(p % nzi);
+    const long long q = p / nzi;
+    const int j = (int)(q % P.ny);
+    const int i = (int)(q / P.ny);
+    double xa, ya, za;
+    arrival_point<C>(P, i, j, k, xa, ya, za);
+    double us0, vs0, ws0;
+    sample3(P, M, xa, ya, za, us0, vs0, ws0);
+    trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd[p], yd[p], zd[p]);
+}
+
+template <int C, int O>
+__global__ void __launch_bounds__(kThreads) k_interp(SlcParams P, NodeView<double> F,
+                                                     const double *x, const double *y,
+                                                     const double *z, long long n, int count_clamp,
+                                                     double *out, unsigned long long *nclamp)
+{
+    const long long p = (long long)blockIdx.x * kThreads + threadIdx.x;
+    unsigned ncl = 0;
+    if (p < n) {
+        double zz = z[p];
+        if (count_clamp) {
+            if (zz < P.z_lo || zz > P.z_hi) ncl = 1;
+            zz = clampz(P, zz);
+        }
+        int c = face_cell(P, zz);
+        Stencil<O, double> st;
+        build_stencil<C, O, double>(P, F.sx, F.sy, x[p], y[p], zz, c, st);
+        out[p] = gather_sum<O, double, double>(F.p, st);
+    }
+    if (count_clamp) add_clamps(nclamp, ncl);
+}
+
+__global__ void k_face_coord(SlcParams P, const double *z, long long n, double *kf)
+{
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) kf[p] = face_coord(P, z[p]);
+}
+
+__global__ void k_lincomb(const double *__restrict__ a, const double *__restrict__ b, double ca,
+                          double cb, double *__restrict__ out, long long n)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x)
+        out[p] = ca * a[p] + cb * b[p];
+}
+
+inline unsigned blocks_for(long long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+
+Vel3 make_vel(const SlcParams &P, Tri mid, bool node)
+{
+    Vel3 M;
+    if (node) {
+        M.u = node_view<double>(mid.u, P.ny, P.nz + 2);
+        M.v = node_view<double>(mid.v, P.ny, P.nz + 2);
+        M.w = node_view<double>(mid.w, P.ny, P.nz + 1);
+    } else {
+        M.u = ghost_view<double>(0, mid.u, P.nx, P.ny, P.nz);
+        M.v = ghost_view<double>(1, mid.v, P.nx, P.ny, P.nz);
+        M.w = ghost_view<double>(2, mid.w, P.nx, P.ny, P.nz);
+    }
+    return M;
+}
+
+template <int O, int MODE>
+void launch_sl_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
+                 unsigned long long *ncl, cudaStream_t s)
+{
+    const long long nc = (long long)P.nx * P.ny * P.nz;
+    const long long nw = (long long)P.nx * P.ny * (P.nz - 1);
+    k_sl<0, O, MODE><<<blocks_for(nc), kThreads, 0, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl);
+    k_sl<1, O, MODE><<<blocks_for(nc), kThreads, 0, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl);
+    if (nw > 0)
+        k_sl<2, O, MODE><<<blocks_for(nw), kThreads, 0, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl);
+    count_launches(nw > 0 ? 3 : 2);
+}
+
+}  // namespace
+
+cudaError_t launch_sl(const SlcParams &P, int mode, Tri fn, Tri fnm1, Tri mid, bool mid_node,
+                      double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s)
+{
+    const Vel3 M = make_vel(P, mid, mid_node);
+    if (P.order == 4) {
+        if (mode == 0) launch_sl_t<4, 0>(P, M, fn, fnm1, dt, out, nclamp, s);
+        else if (mode == 1) launch_sl_t<4, 1>(P, M, fn, fnm1, dt, out, nclamp, s);
+        else launch_sl_t<4, 2>(P, M, fn, fnm1, dt, out, nclamp, s);
+    } else {
+        if (mode == 0) launch_sl_t<6, 0>(P, M, fn, fnm1, dt, out, nclamp, s);
+        else if (mode == 1) launch_sl_t<6, 1>(P, M, fn, fnm1, dt, out, nclamp, s);
+        else launch_sl_t<6, 2>(P, M, fn, fnm1, dt, out, nclamp, s);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_departure(const SlcParams &P, int comp, Tri mid_node, double dt, double *xd,
+                             double *yd, double *zd, cudaStream_t s)
+{
+    const Vel3 M = make_vel(P, mid_node, true);
+    const long long n = (long long)P.nx * P.ny * (comp == 2 ? P.nz - 1 : P.nz);
+    if (n <= 0) return cudaSuccess;
+    if (comp == 0) k_departure<0><<<blocks_for(n), kThreads, 0, s>>>(P, M, dt, xd, yd, zd);
+    else if (comp == 1) k_departure<1><<<blocks_for(n), kThreads, 0, s>>>(P, M, dt, xd, yd, zd);
+    else k_departure<2><<<blocks_for(n), kThreads, 0, s>>>(P, M, dt, xd, yd, zd);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+namespace {
+template <int C>
+void launch_interp_c(const SlcParams &P, int order, NodeView<double> F, const double *x,
+                     const double *y, const double *z, long long n, int cc, double *out,
+                     unsigned long long *ncl, cudaStream_t s)
+{
+    if (order == 2) k_interp<C, 2><<<blocks_for(n), kThreads, 0, s>>>(P, F, x, y, z, n, cc, out, ncl);
+    else if (order == 4) k_interp<C, 4><<<blocks_for(n), kThreads, 0, s>>>(P, F, x, y, z, n, cc, out, ncl);
+    else k_interp<C, 6><<<blocks_for(n), kThreads, 0, s>>>(P, F, x, y, z, n, cc, out, ncl);
+}
+}  // namespace
+
+cudaError_t launch_interp(const SlcParams &P, int comp, int order, const double *buf,
+                          const double *x, const double *y, const double *z, int64_t n,
+                          int count_clamp, double *out, unsigned long long *nclamp,
+                          cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    const int NZ = comp == 2 ? P.nz + 1 : P.nz + 2;
+    const NodeView<double> F = node_view<double>(buf, P.ny, NZ);
+    if (comp == 0) launch_interp_c<0>(P, order, F, x, y, z, n, count_clamp, out, nclamp, s);
+    else if (comp == 1) launch_interp_c<1>(P, order, F, x, y, z, n, count_clamp, out, nclamp, s);
+    else launch_interp_c<2>(P, order, F, x, y, z, n, count_clamp, out, nclamp, s);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_face_coord(const SlcParams &P, const double *z, int64_t n, double *kf,
+                              cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    k_face_coord<<<blocks_for(n), kThreads, 0, s>>>(P, z, n, kf);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lincomb(const double *a, const double *b, double ca, double cb, double *out,
+                           int64_t n, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    unsigned blocks = blocks_for(n);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_lincomb<<<blocks, kThreads, 0, s>>>(a, b, ca, cb, out, n);
+    count_launches(1);
+    return cudaGetLastError();
+}

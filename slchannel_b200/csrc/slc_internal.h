@@ -1,0 +1,70 @@
+// slc_internal.h -- launch wrappers shared between the .cu files of the
+// library (not part of the public ABI; see include/slc_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+
+#include "slc_common.cuh"
+
+// Number of this library's kernel launches (slc_kernel_launches()).
+extern std::atomic<long long> g_slc_launches;
+inline void count_launches(int n) { g_slc_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Raw pointers of a velocity triple (ghost-shaped arrays or node buffers).
+struct Tri {
+    const double *u, *v, *w;
+};
+struct TriMut {
+    double *u, *v, *w;
+};
+
+// ---- sl_trace_gather.cu ----------------------------------------------------
+// mode: 0 = one foot (advect), 1 = BDF1 predictor, 2 = BDF2 predictor.
+// `mid_node` selects the layout of `mid`: true = node buffers (NX, NY, NZ),
+// false = ghost-shaped arrays.
+cudaError_t launch_sl(const SlcParams &P, int mode, Tri fn, Tri fnm1, Tri mid, bool mid_node,
+                      double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s);
+cudaError_t launch_departure(const SlcParams &P, int comp, Tri mid_node, double dt, double *xd,
+                             double *yd, double *zd, cudaStream_t s);
+cudaError_t launch_interp(const SlcParams &P, int comp, int order, const double *buf,
+                          const double *x, const double *y, const double *z, int64_t n,
+                          int count_clamp, double *out, unsigned long long *nclamp,
+                          cudaStream_t s);
+cudaError_t launch_face_coord(const SlcParams &P, const double *z, int64_t n, double *kf,
+                              cudaStream_t s);
+cudaError_t launch_lincomb(const double *a, const double *b, double ca, double cb, double *out,
+                           int64_t n, cudaStream_t s);
+
+// ---- zsolve.cu ---------------------------------------------------------------
+// Thomas factorisation tables of (I - dt nu Dzz) with the wall closures:
+// tab_uv = [alpha(nz) | invden(nz) | cprime(nz)], tab_w likewise with nz-1.
+cudaError_t launch_zsolve_tables(const SlcParams &P, const double *dz_c, const double *dz_f,
+                                 double dt, double *tab_uv, double *tab_w, cudaStream_t s);
+cudaError_t launch_zsolve(const SlcParams &P, TriMut f, const double *tab_uv, const double *tab_w,
+                          cudaStream_t s);
+
+// ---- poisson.cu --------------------------------------------------------------
+cudaError_t launch_apply_bc(const SlcParams &P, double *u, double *v, double *w, double *p,
+                            cudaStream_t s);
+cudaError_t launch_div_pack(const SlcParams &P, Tri f, const double *dz_f, double dt_div,
+                            double *rhs_zmajor, cudaStream_t s);
+cudaError_t launch_divergence(const SlcParams &P, Tri f, const double *dz_f, double *div,
+                              cudaStream_t s);
+cudaError_t launch_thomas_poisson(const SlcParams &P, double *hat, double *cp, const double *kx2,
+                                  const double *ky2, const double *cl, const double *cr,
+                                  cudaStream_t s);
+cudaError_t launch_project(const SlcParams &P, const double *phi_zmajor, TriMut f, double *p,
+                           const double *dz_c, double dt, cudaStream_t s);
+// bulk: partial sums of u*dz_f over the interior (shift c added first when
+// c_dev != NULL), then a fixed-order finish.  out[0] = bulk; with
+// shift_out != NULL: shift_out[0] = U_bulk - bulk, shift_out[1] = that / dt.
+cudaError_t launch_bulk_partials(const SlcParams &P, double *u, const double *dz_f,
+                                 const double *c_dev, double *partials, cudaStream_t s);
+cudaError_t launch_bulk_finish(const SlcParams &P, const double *partials, double Lx, double Ly,
+                               double U_bulk, double dt, double *bulk_out, double *shift_out,
+                               cudaStream_t s);
+
+constexpr int kBulkBlocks = 296;  // 2 x 148 SMs, fixed for a deterministic sum

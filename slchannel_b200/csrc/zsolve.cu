@@ -1,0 +1,182 @@
+// zsolve.cu -- theta = 1 implicit wall-normal diffusion (I - dt nu Dzz) f = rhs
+// on every (i, j) column of u, v and w, in place on the interiors.
+//
+// The diagonals are the reference's (operators.py:382-630: interior rows from
+// dz_c / dz_f, no-slip or free-slip wall closures for u, v; w rows dropping the
+// wall couplings).  They are the same for every column, so the Thomas
+// factorisation (denominators and c') is computed once per dt by one thread,
+// and each column is solved by one warp: lane l owns a contiguous chunk of the
+// column in registers, the forward recurrence d'_k = alpha_k d'_{k-1} +
+// invden_k d_k and the backward recurrence x_k = -c'_k x_{k+1} + d'_k are
+// affine maps, and a 5-step warp scan of the per-chunk maps hands each lane
+// its incoming value.  The reference solves the same systems with parallel
+// cyclic reduction (tridiag.py:36-61); the results agree to rounding.
+#include "slc_internal.h"
+
+namespace {
+
+// One thread per system (0: u/v, 1: w); sequential factorisation.
+__global__ void k_zsolve_tables(SlcParams P, const double *dz_c, const double *dz_f, double dt,
+                                double *tab_uv, double *tab_w)
+{
+    const int which = threadIdx.x;
+    if (which > 1) return;
+    const double alpha = 1.0 * dt * P.nu;  // theta = 1
+    const int nz = P.nz;
+    const int n = which == 0 ? nz : nz - 1;
+    if (n <= 0) return;
+    double *al = which == 0 ? tab_uv : tab_w;
+    double *inv = al + n;
+    double *cp = inv + n;
+    double cprev = 0.0;
+    for (int k = 0; k < n; ++k) {
+        double dl, dr, dc;
+        if (which == 0) {
+            dl = dz_c[k];
+            dr = dz_c[k + 1];
+            dc = dz_f[k];
+        } else {
+            dl = dz_f[k];
+            dr = dz_f[k + 1];
+            dc = dz_c[k + 1];
+        }
+        const double lower = -alpha / (dl * dc);
+        const double center = 1.0 + alpha * (1.0 / dl + 1.0 / dr) / dc;
+        const double upper = -alpha / (dr * dc);
+        double a = lower, b = center, c = upper;
+        if (k == 0) {
+            a = 0.0;
+            if (which == 0) b = center - lower;  // u[0] = -u[1]
+        }
+        if (k == n - 1) {
+            c = 0.0;
+            if (which == 0) b = P.top_neumann ? center + upper : center - upper;
+        }
+        const double denom = b - a * cprev;
+        const double id = 1.0 / denom;
+        const double cpk = c * id;
+        al[k] = -a * id;
+        inv[k] = id;
+        cp[k] = cpk;
+        cprev = cpk;
+    }
+}
+
+template <int CH>
+__global__ void __launch_bounds__(256) k_zsolve(SlcParams P, double *u, double *v, double *w,
+                                                const double *__restrict__ tab_uv,
+                                                const double *__restrict__ tab_w)
+{
+    const int lane = threadIdx.x & 31;
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long ncol = (long long)P.nx * P.ny;
+    if (wid >= 3 * ncol) return;  // whole warps exit together
+    const int comp = (int)(wid / ncol);
+    const long long col = wid % ncol;
+    const int i = (int)(col / P.ny), j = (int)(col % P.ny);
+    const GhostShape g = ghost_shape(comp, P.nx, P.ny, P.nz);
+    double *base = comp == 0 ? u : (comp == 1 ? v : w);
+    double *colp = base + (size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + 1;
+    const int n = comp == 2 ? P.nz - 1 : P.nz;
+    const double *tab = comp == 2 ? tab_w : tab_uv;
+    const double *al = tab, *inv = tab + n, *cp = tab + 2 * n;
+
+    const int s = lane * CH;
+    double d[CH];
+#pragma unroll
+    for (int q = 0; q < CH; ++q) d[q] = (s + q < n) ? colp[s + q] : 0.0;
+
+    // forward: chunk map y_out = A y_in + B
+    double A = 1.0, B = 0.0;
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+        const int k = s + q;
+        if (k < n) {
+            const double a = __ldg(al + k);
+            B = fma(a, B, __ldg(inv + k) * d[q]);
+            A = a * A;
+        }
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double Ap = __shfl_up_sync(0xffffffffu, A, off);
+        const double Bp = __shfl_up_sync(0xffffffffu, B, off);
+        if (lane >= off) {
+            B = fma(A, Bp, B);
+            A = A * Ap;
+        }
+    }
+    double y = __shfl_up_sync(0xffffffffu, B, 1);
+    if (lane == 0) y = 0.0;
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+        const int k = s + q;
+        if (k < n) {
+            y = fma(__ldg(al + k), y, __ldg(inv + k) * d[q]);
+            d[q] = y;
+        }
+    }
+
+    // backward: x_k = -c'_k x_{k+1} + d'_k (c'_{n-1} = 0)
+    A = 1.0;
+    B = 0.0;
+#pragma unroll
+    for (int q = CH - 1; q >= 0; --q) {
+        const int k = s + q;
+        if (k < n) {
+            const double gk = -__ldg(cp + k);
+            B = fma(gk, B, d[q]);
+            A = gk * A;
+        }
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double An = __shfl_down_sync(0xffffffffu, A, off);
+        const double Bn = __shfl_down_sync(0xffffffffu, B, off);
+        if (lane + off < 32) {
+            B = fma(A, Bn, B);
+            A = A * An;
+        }
+    }
+    double x = __shfl_down_sync(0xffffffffu, B, 1);
+    if (lane == 31) x = 0.0;
+#pragma unroll
+    for (int q = CH - 1; q >= 0; --q) {
+        const int k = s + q;
+        if (k < n) {
+            x = fma(-__ldg(cp + k), x, d[q]);
+            d[q] = x;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < CH; ++q)
+        if (s + q < n) colp[s + q] = d[q];
+}
+
+}  // namespace
+
+cudaError_t launch_zsolve_tables(const SlcParams &P, const double *dz_c, const double *dz_f,
+                                 double dt, double *tab_uv, double *tab_w, cudaStream_t s)
+{
+    k_zsolve_tables<<<1, 32, 0, s>>>(P, dz_c, dz_f, dt, tab_uv, tab_w);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zsolve(const SlcParams &P, TriMut f, const double *tab_uv, const double *tab_w,
+                          cudaStream_t s)
+{
+    const long long warps = 3LL * P.nx * P.ny;
+    const unsigned blocks = (unsigned)((warps * 32 + 255) / 256);
+    const int need = (P.nz + 31) / 32;  // chunk length per lane
+    if (need <= 1) k_zsolve<1><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+    else if (need <= 2) k_zsolve<2><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+    else if (need <= 4) k_zsolve<4><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+    else if (need <= 8) k_zsolve<8><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+    else if (need <= 12) k_zsolve<12><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+    else if (need <= 16) k_zsolve<16><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+    else if (need <= 32) k_zsolve<32><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+    else return cudaErrorInvalidValue;  // nz > 1024
+    count_launches(1);
+    return cudaGetLastError();
+}

@@ -1,0 +1,276 @@
+"""SLChannelFlow: drop-in for slchannel.solver.SLChannelFlow's SL-BDF2 step.
+
+Reads the reference's YAML surface (slchannel/solver.py:168-282,
+docs/CONFIG.md), builds the grid and the initial field, and advances it with
+``step_sl_bdf2`` (solver.py:813-1018) -- Boukir BDF2 along characteristics,
+theta = 1 wall-normal diffusion, FFT pressure projection and the exact
+bulk-flux shift -- executed by libslc_b200.so on one GPU.  The fields
+``u, v, w, p`` and the history ``u_nm1, v_nm1, w_nm1`` are ghost-shaped
+float64 CUDA tensors, exactly as in the reference; between steps they are
+BC-consistent.
+
+The time loop / output shell of the reference (run_simulation,
+solver.py:1140-1637) and the Eulerian comparison scheme are not part of this
+package.
+"""
+
+from __future__ import annotations
+
+import torch
+import yaml
+
+from . import _native as N
+from .initflow import initialize_flow, initialize_flow_from_file
+from .semilag import SLAdvector
+from .utils import compute_bulk_velocity, compute_divergence, generate_grid
+
+
+class SLChannelFlow:
+    """Channel-flow DNS driver with the SL-BDF2 step on a B200."""
+
+    def __init__(self, config_file="config.yaml", allocate_fields=True, *, config=None):
+        if config is None:
+            with open(config_file, "r") as f:
+                config = yaml.safe_load(f)
+        self.config = config
+
+        dev_cfg = config.get("compute", {}).get("device", "auto")
+        if dev_cfg == "cpu":
+            raise RuntimeError("slchannel_b200 runs on a CUDA device (sm_100a); there is no CPU path")
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDA requested but not available")
+        self.device = torch.device("cuda", torch.cuda.current_device())
+
+        self.nx = config["grid"]["nx"]
+        self.ny = config["grid"]["ny"]
+        self.nz = config["grid"]["nz"]
+        self.Lx = config["domain"]["Lx"]
+        self.Ly = config["domain"]["Ly"]
+        self.Lz = config["domain"]["Lz"]
+        self.stretching_type = config["domain"].get("stretching_type", "symmetric")
+        if self.stretching_type not in ["symmetric", "bottom"]:
+            raise ValueError(
+                f"Invalid stretching type: {self.stretching_type}. "
+                "slChannel supports 'symmetric' or 'bottom'")
+        self.nu = 1.0 / config["flow"]["Re"]
+        self.Re_tau = config["flow"].get("Re_tau", 180.0)
+        self.U_bulk = config["flow"]["U_bulk"]
+        self.gamma = config["flow"]["gamma"]
+        bc_config = config.get("boundary_conditions", {})
+        self.top_wall_bc_type = bc_config.get("top_wall", {}).get("type", "dirichlet")
+        if self.top_wall_bc_type not in ["dirichlet", "neumann"]:
+            raise ValueError(f"Invalid top wall BC type: {self.top_wall_bc_type}")
+        t = config.get("time", {})
+        self.dt = t.get("dt", 0.01)
+        self.n_steps = t.get("n_steps", 0)
+        self.t_max = t.get("t_max", 1000.0)
+        self.dt_update_interval = t.get("dt_update_interval", 0)
+
+        self.advection_scheme = config.get("advection", {}).get("scheme", "sl")
+        if self.advection_scheme not in ["sl", "eulerian"]:
+            raise ValueError(
+                f"advection.scheme must be 'sl' or 'eulerian', got {self.advection_scheme}")
+        if self.advection_scheme != "sl":
+            raise NotImplementedError("slchannel_b200 implements the 'sl' scheme only")
+        sl_cfg = config.get("sl", {})
+        self.sl_order = sl_cfg.get("interp_order", 4)
+        if self.sl_order not in (4, 6):
+            raise ValueError(
+                f"sl.interp_order must be 4 (tricubic) or 6 (triquintic), got {self.sl_order}")
+        self.sl_traj_order = sl_cfg.get("traj_interp_order", 2)
+        self.sl_traj_iters = sl_cfg.get("n_traj_iters", 2)
+        self.sl_interp_dtype = sl_cfg.get("interp_dtype", "fp64")
+        self.sl_bdf2_pressure = sl_cfg.get("bdf2_pressure", "noninc")
+        self.sl_bdf2_xy_rhs = sl_cfg.get("bdf2_xy_rhs", "extrap")
+        for removed in ("time_scheme", "traj_extrapolation", "field_interp"):
+            if removed in sl_cfg:
+                raise ValueError(
+                    f"sl.{removed} was removed in the bdf2-only cleanup: the SL scheme is always "
+                    f"Boukir BDF2 characteristics now (drop the key from the config)")
+        if self.sl_bdf2_pressure not in ["noninc", "inc"]:
+            raise ValueError(
+                f"sl.bdf2_pressure must be 'noninc' or 'inc', got {self.sl_bdf2_pressure}")
+        if self.sl_bdf2_xy_rhs not in ["extrap", "lagged"]:
+            raise ValueError(
+                f"sl.bdf2_xy_rhs must be 'extrap' or 'lagged', got {self.sl_bdf2_xy_rhs}")
+        if self.sl_bdf2_pressure == "inc":
+            raise NotImplementedError("sl.bdf2_pressure 'inc' is not implemented on the GPU path")
+        solver_type = config.get("solver", {}).get("type", "fft")
+        if solver_type != "fft":
+            raise ValueError(f"solver.type must be 'fft', got {solver_type!r}.")
+
+        out_cfg = config.get("output", {})
+        self.results_folder = out_cfg.get("results_folder", "results")
+        self.allocate_fields = allocate_fields
+
+        torch.set_default_dtype(torch.float64)
+        self.z_f, self.z_c, self.dz_f, self.dz_c = generate_grid(
+            self.gamma, self.nz, self.Lz, device=self.device, stretching_type=self.stretching_type)
+        self.dx = self.Lx / self.nx
+        self.dy = self.Ly / self.ny
+        self.cell_vol = (self.dx * self.dy * self.dz_f.view(1, 1, -1)).expand(self.nx, self.ny, self.nz)
+        self.cell_vol_ratio = self.cell_vol
+        self.total_volume = self.Lx * self.Ly * self.Lz
+
+        self.sl = SLAdvector(
+            self.nx, self.ny, self.nz, self.dx, self.dy, self.Lx, self.Ly, self.Lz,
+            self.z_f, self.z_c, self.gamma, stretching_type=self.stretching_type,
+            order=self.sl_order, traj_order=self.sl_traj_order, n_traj_iters=self.sl_traj_iters,
+            top_wall_bc_type=self.top_wall_bc_type, interp_dtype=self.sl_interp_dtype,
+            device=self.device, nu=self.nu, xy_rhs=self.sl_bdf2_xy_rhs)
+        self._grid = self.sl.native
+
+        init_cfg = config.get("initialization", {})
+        field_file = init_cfg.get("field_file", None)
+        self.forcing = 0.0
+        self.initial_step, self.time = 0, 0.0
+        if not allocate_fields:
+            self.u = self.v = self.w = self.p = None
+        elif field_file is not None and init_cfg.get("type", "parabolic") != "interpolate":
+            self.u, self.v, self.w, self.p, self.initial_step, self.time = initialize_flow_from_file(
+                field_file, device=self.device, reset_time=init_cfg.get("reset_time", False))
+        else:
+            self.u, self.v, self.w, self.p = initialize_flow(
+                self.nx, self.ny, self.nz, self.z_c, self.Ly, self.Lz, U_bulk=self.U_bulk,
+                init_type=init_cfg.get("type", "parabolic"),
+                perturbation_intensity=init_cfg.get("perturbation_intensity", 0.0),
+                n_vortices=init_cfg.get("n_vortices", 4), device=self.device,
+                top_wall_bc_type=self.top_wall_bc_type)
+            ub = float(compute_bulk_velocity(self.u, self.cell_vol_ratio, self.total_volume))
+            if abs(ub) > 1e-9:
+                self.u *= self.U_bulk / ub
+        self.initial_time = self.time
+        self.current_step = self.initial_step
+
+        self.u_nm1 = self.v_nm1 = self.w_nm1 = None
+        self._next = None
+        self._dt_prev_step = None
+        if allocate_fields:
+            self._save_and_project_initial()
+
+    # ------------------------------------------------------------------
+    def _stream(self):
+        return N.stream_of(self.u)
+
+    def _check_state(self):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        N.require(self.u, (nx + 1, ny + 2, nz + 2), "u")
+        N.require(self.v, (nx + 2, ny + 1, nz + 2), "v")
+        N.require(self.w, (nx + 2, ny + 2, nz + 1), "w")
+        N.require(self.p, (nx + 2, ny + 2, nz + 2), "p")
+
+    def apply_bc_uvw(self):
+        """solver.py:646-647 -> apply_bc_all (solver.py:70-107), on the GPU."""
+        self._grid.call("slc_apply_bc", N.ptr(self.u), N.ptr(self.v), N.ptr(self.w), self._stream())
+
+    def _project(self, dt_div, dt_proj):
+        self._grid.call("slc_project", N.ptr(self.u), N.ptr(self.v), N.ptr(self.w), N.ptr(self.p),
+                        float(dt_div), float(dt_proj), self._stream())
+
+    def _save_and_project_initial(self):
+        """solver.py:593-625 -- project the initial field (dt = 1)."""
+        self._check_state()
+        self.apply_bc_uvw()
+        self._project(1.0, 1.0)
+
+    def set_state(self, u, v, w, p=None):
+        """Replace the velocity (and pressure) with caller-given ghost-shaped
+        arrays and drop the BDF2 history (the next step re-bootstraps, as a
+        restart does in the reference)."""
+        f = dict(device=self.device, dtype=torch.float64)
+        self.u = torch.as_tensor(u).to(**f).contiguous().clone()
+        self.v = torch.as_tensor(v).to(**f).contiguous().clone()
+        self.w = torch.as_tensor(w).to(**f).contiguous().clone()
+        if p is not None:
+            self.p = torch.as_tensor(p).to(**f).contiguous().clone()
+        self.u_nm1 = self.v_nm1 = self.w_nm1 = None
+        self._next = None
+        self._dt_prev_step = None
+        self._check_state()
+
+    def compute_divergence(self):
+        return compute_divergence(self.u, self.v, self.w, self.nx, self.ny, self.nz, self.dx,
+                                  self.dy, self.dz_f)
+
+    # ------------------------------------------------------------------
+    # SL-BDF2
+    # ------------------------------------------------------------------
+    def _apply_bulk_forcing(self, dt):
+        """solver.py:694-723 -- exact uniform shift of u to the target bulk
+        velocity; returns (u_bulk after the shift, forcing = shift / dt) as
+        0-D device tensors."""
+        out = torch.empty(2, dtype=torch.float64, device=self.device)
+        self._grid.call("slc_bulk_shift", N.ptr(self.u), N.ptr(self.v), N.ptr(self.w),
+                        float(self.U_bulk), float(dt), N.ptr(out), self._stream())
+        self.forcing = out[1]
+        return out[0], out[1]
+
+    def _bdf2_forcing_update(self, dt):
+        return self._apply_bulk_forcing(dt)
+
+    def _alloc_next(self):
+        return (torch.zeros_like(self.u), torch.zeros_like(self.v), torch.zeros_like(self.w))
+
+    def _step_sl_bdf1_bootstrap(self, dt, dt_t=None):
+        """solver.py:729-811 -- one BDF1 characteristics step; seeds the
+        history (V^{n-1} <- V^n)."""
+        self._check_state()
+        nxt = self._next if self._next is not None else self._alloc_next()
+        cur = (self.u, self.v, self.w)
+        pc, kc = N.ptr_array(cur)
+        pn, kn = N.ptr_array(nxt)
+        self._grid.call("slc_step_bdf1", pc, pn, N.ptr(self.p), float(dt),
+                        N.ptr(self.sl.n_clamped_last), self._stream())
+        old = (self.u_nm1, self.v_nm1, self.w_nm1)
+        self.u_nm1, self.v_nm1, self.w_nm1 = cur
+        self.u, self.v, self.w = nxt
+        self._next = old if old[0] is not None else None
+        self._dt_prev_step = dt
+        return self._bdf2_forcing_update(dt)
+
+    def step_sl_bdf2(self, dt):
+        """solver.py:813-1018 -- one SL-BDF2 step (BDF1 bootstrap on the
+        first step, after set_state and whenever dt changes).  Returns
+        (u_bulk, forcing) as 0-D device tensors."""
+        dt = float(dt)
+        if (self.u_nm1 is None or self._dt_prev_step is None
+                or abs(dt - self._dt_prev_step) > 1e-12 * dt):
+            if self._dt_prev_step is not None and self.u_nm1 is not None:
+                print(f"[bdf2] dt changed ({self._dt_prev_step:.6g} -> {dt:.6g}): BDF1 re-bootstrap",
+                      flush=True)
+            return self._step_sl_bdf1_bootstrap(dt)
+        self._check_state()
+        if self._next is None:
+            self._next = self._alloc_next()
+        cur = (self.u, self.v, self.w)
+        prev = (self.u_nm1, self.v_nm1, self.w_nm1)
+        nxt = self._next
+        pc, kc = N.ptr_array(cur)
+        pp, kp = N.ptr_array(prev)
+        pn, kn = N.ptr_array(nxt)
+        self._grid.call("slc_step_bdf2", pc, pp, pn, N.ptr(self.p), dt,
+                        N.ptr(self.sl.n_clamped_last), self._stream())
+        self.u_nm1, self.v_nm1, self.w_nm1 = cur
+        self.u, self.v, self.w = nxt
+        self._next = prev
+        self._dt_prev_step = dt
+        return self._bdf2_forcing_update(dt)
+
+    def run_steps(self, n, dt=None):
+        """Advance n SL-BDF2 steps at fixed dt (default: time.dt); returns the
+        last (u_bulk, forcing)."""
+        dt = self.dt if dt is None else dt
+        res = None
+        for _ in range(int(n)):
+            res = self.step_sl_bdf2(dt)
+            self.time += dt
+            self.current_step += 1
+        return res
+
+
+def load_config(path):
+    with open(path) as f:
+        return yaml.safe_load(f)
+
+
+__all__ = ["SLChannelFlow", "load_config"]

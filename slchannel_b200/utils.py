@@ -1,0 +1,74 @@
+"""Grid construction and the step diagnostics (reference: slchannel/utils.py).
+
+``generate_grid`` is init-time host code (the reference's formulas, float64);
+``compute_divergence`` and ``compute_bulk_velocity`` run as CUDA kernels of
+libslc_b200.so and return device tensors.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import _native as N
+
+
+def generate_grid(gamma, nz, Lz, device="cpu", stretching_type="symmetric"):
+    """utils.py:21-61 -- tanh-stretched faces z_f (nz+1), centres z_c with the
+    two mirrored ghost centres (nz+2), dz_f (nz) and dz_c (nz+1), float64.
+
+    Evaluated on the host (init only) and moved to `device`."""
+    k = torch.linspace(0, nz, nz + 1, dtype=torch.float64)
+    g = torch.tensor(gamma, dtype=torch.float64)
+    if stretching_type == "bottom":
+        xi = k / nz
+        z_f = Lz * (1.0 - torch.tanh(gamma * (1.0 - xi)) / torch.tanh(g))
+    else:
+        xi = (2 * k / nz) - 1
+        z_f = 0.5 * Lz * (1 + torch.tanh(gamma * xi) / torch.tanh(g))
+    z_c_inn = 0.5 * (z_f[:-1] + z_f[1:])
+    z_c = torch.cat([-z_c_inn[:1], z_c_inn, (2 * z_f[-1] - z_c_inn[-1]).reshape(1)])
+    dz_f = z_f[1:] - z_f[:-1]
+    dz_c = z_c[1:] - z_c[:-1]
+    return tuple(t.to(device) for t in (z_f, z_c, dz_f, dz_c))
+
+
+def field_shapes(nx, ny, nz):
+    return {"u": (nx + 1, ny + 2, nz + 2), "v": (nx + 2, ny + 1, nz + 2),
+            "w": (nx + 2, ny + 2, nz + 1), "p": (nx + 2, ny + 2, nz + 2)}
+
+
+def compute_divergence(u, v, w, nx, ny, nz, dx, dy, dz_f):
+    """utils.py:166-180 -- divergence of the staggered field, (nx, ny, nz)."""
+    sh = field_shapes(nx, ny, nz)
+    N.require(u, sh["u"], "u")
+    N.require(v, sh["v"], "v")
+    N.require(w, sh["w"], "w")
+    dz = dz_f.to(device=u.device, dtype=torch.float64).contiguous()
+    if dz.numel() < nz:
+        raise ValueError("dz_f must have nz entries")
+    div = torch.empty((nx, ny, nz), dtype=torch.float64, device=u.device)
+    rc = N.lib().slc_divergence_raw(nx, ny, nz, float(dx), float(dy), N.ptr(dz), N.ptr(u),
+                                    N.ptr(v), N.ptr(w), N.ptr(div), N.stream_of(u))
+    N.check(rc)
+    return div
+
+
+def compute_bulk_velocity(u, cell_vol_ratio, total_volume):
+    """utils.py:147-163 -- sum(u_int * cell_vol) / V as a 0-D device tensor.
+
+    `cell_vol_ratio` is the solver's (nx, ny, nz) cell-volume tensor
+    dx*dy*dz_f expanded over x and y (solver.py:303-306); its per-level
+    column is what the kernel reads."""
+    nx, ny, nz = cell_vol_ratio.shape
+    N.require(u, (nx + 1, ny + 2, nz + 2), "u")
+    vol_k = cell_vol_ratio[0, 0, :].to(device=u.device, dtype=torch.float64).contiguous()
+    if cell_vol_ratio.stride()[:2] != (0, 0) and not torch.equal(
+            cell_vol_ratio.to(vol_k.device), vol_k.view(1, 1, nz).expand(nx, ny, nz)):
+        raise ValueError("cell_vol_ratio must be constant over x and y (dx*dy*dz_f)")
+    scratch = torch.empty(N.lib().slc_bulk_scratch_doubles(), dtype=torch.float64, device=u.device)
+    out = torch.empty((), dtype=torch.float64, device=u.device)
+    rc = N.lib().slc_bulk_velocity_raw(nx, ny, nz, N.ptr(u), N.ptr(vol_k),
+                                       1.0 / float(total_volume), N.ptr(scratch), N.ptr(out),
+                                       N.stream_of(u))
+    N.check(rc)
+    return out
