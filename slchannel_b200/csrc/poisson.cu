@@ -126,8 +126,8 @@ __device__ __forceinline__ double div_at(const SlcParams &P, const double *__res
     const size_t wsx = (size_t)(ny + 2) * (nz + 1), wsy = nz + 1;
     const int im = i == 0 ? nx : i;  // u row i (0-based interior i-1) ; ghost row 0 == row nx
     const int jm = j == 0 ? ny : j;
-    const double du = (u[(i + 1) * usx + (j + 1) * usy + k + 1] - u[im * usx + (j + 1) * usy + k + 1]) / P.dx;
-    const double dv = (v[(i + 1) * vsx + (j + 1) * vsy + k + 1] - v[(i + 1) * vsx + jm * vsy + k + 1]) / P.dy;
+    const double du = (u[(i + 1) * usx + (j + 1) * usy + k + 1] - u[im * usx + (j + 1) * usy + k + 1]) * P.inv_dx;
+    const double dv = (v[(i + 1) * vsx + (j + 1) * vsy + k + 1] - v[(i + 1) * vsx + jm * vsy + k + 1]) * P.inv_dy;
     const double dw = (w[(i + 1) * wsx + (j + 1) * wsy + k + 1] - w[(i + 1) * wsx + (j + 1) * wsy + k]) / dz_f[k];
     return du + dv + dw;
 }
@@ -177,55 +177,90 @@ __global__ void k_divergence(SlcParams P, const double *__restrict__ u,
 // substitution.
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) k_thomas(SlcParams P, double2 *__restrict__ hat,
+constexpr int kPre = 8;  // loads kept in flight per thread in the sweeps
+
+__global__ void __launch_bounds__(256) k_thomas(SlcParams P, double *__restrict__ hat,
                                                 double *__restrict__ cpw,
                                                 const double *__restrict__ kx2,
                                                 const double *__restrict__ ky2,
                                                 const double *__restrict__ cl,
                                                 const double *__restrict__ cr, double norm)
 {
+    // thread t handles part (t & 1) (0 real, 1 imaginary) of column t >> 1; the
+    // coefficients are real, so the two parts are independent systems.  The
+    // real-part thread stores c' (same values in both), read back by both after
+    // a warp barrier.
     const int nky = P.ny / 2 + 1;
-    const long long ncol = (long long)P.nx * nky;
-    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
+    const int ncol = P.nx * nky;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int col = t >> 1, part = t & 1;
+    const bool active = col < ncol;
     const int nz = P.nz;
-    const int kx = (int)(col / nky), ky = (int)(col % nky);
-    const double k2 = kx2[kx] + ky2[ky];
-    const size_t st = (size_t)ncol;
-
-    double b = -(cl[0] + cr[0] + k2) + cl[0];
-    if (nz == 1) b += cr[0];
-    double c = nz > 1 ? cr[0] : 0.0;
-    if (col == 0) {
-        b = 1.0;
-        c = 0.0;
+    const size_t st = 2 * (size_t)ncol;  // doubles per k-plane of the spectrum
+    double *h = hat + 2 * (size_t)(active ? col : 0) + part;
+    double *cpc = cpw + (active ? col : 0);
+    double k2 = 0.0;
+    if (active) {
+        const int kx = col / nky, ky = col - (col / nky) * nky;
+        k2 = kx2[kx] + ky2[ky];
     }
-    double id = 1.0 / b;
-    double cprev = c * id;
-    double2 d = hat[col];
-    double2 dp = make_double2(d.x * id, d.y * id);
-    hat[col] = dp;
-    cpw[col] = cprev;
-    for (int k = 1; k < nz; ++k) {
-        const double a = cl[k];
-        double bk = -(cl[k] + cr[k] + k2);
-        if (k == nz - 1) bk += cr[nz - 1];
-        const double ck = (k < nz - 1) ? cr[k] : 0.0;
-        const double denom = bk - a * cprev;
-        id = 1.0 / denom;
-        cprev = ck * id;
-        d = hat[k * st + col];
-        dp = make_double2((d.x - a * dp.x) * id, (d.y - a * dp.y) * id);
-        hat[k * st + col] = dp;
-        cpw[k * st + col] = cprev;
+    double buf[kPre];
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < kPre; ++q) buf[q] = q < nz ? h[q * st] : 0.0;
+        double cprev = 0.0, dprev = 0.0;
+        for (int k0 = 0; k0 < nz; k0 += kPre) {
+#pragma unroll
+            for (int q = 0; q < kPre; ++q) {
+                const int k = k0 + q;
+                if (k < nz) {
+                    const double d = buf[q];
+                    if (k + kPre < nz) buf[q] = h[(k + kPre) * st];
+                    const double a = k > 0 ? cl[k] : 0.0;
+                    double b = -(cl[k] + cr[k] + k2);
+                    if (k == 0) b += cl[0];
+                    if (k == nz - 1) b += cr[nz - 1];
+                    double c = k < nz - 1 ? cr[k] : 0.0;
+                    if (col == 0 && k == 0) {  // pinned (0,0) mode: identity first row
+                        b = 1.0;
+                        c = 0.0;
+                    }
+                    const double id = 1.0 / (b - a * cprev);
+                    cprev = c * id;
+                    dprev = (d - a * dprev) * id;
+                    h[k * st] = dprev;
+                    if (part == 0) cpc[k * (size_t)ncol] = cprev;
+                }
+            }
+        }
     }
-    double2 x = dp;
-    hat[(size_t)(nz - 1) * st + col] = make_double2(x.x * norm, x.y * norm);
-    for (int k = nz - 2; k >= 0; --k) {
-        const double2 dk = hat[k * st + col];
-        const double ck = cpw[k * st + col];
-        x = make_double2(dk.x - ck * x.x, dk.y - ck * x.y);
-        hat[k * st + col] = make_double2(x.x * norm, x.y * norm);
+    __syncwarp();
+    if (active) {
+        // back substitution, prefetching d' and c' downwards
+        double cb[kPre];
+#pragma unroll
+        for (int q = 0; q < kPre; ++q) {
+            const int k = nz - 1 - q;
+            buf[q] = k >= 0 ? h[k * st] : 0.0;
+            cb[q] = k >= 0 ? cpc[k * (size_t)ncol] : 0.0;
+        }
+        double x = 0.0;
+        for (int r0 = 0; r0 < nz; r0 += kPre) {
+#pragma unroll
+            for (int q = 0; q < kPre; ++q) {
+                const int k = nz - 1 - (r0 + q);
+                if (k >= 0) {
+                    const double dk = buf[q], ck = cb[q];
+                    const int kn = k - kPre;
+                    if (kn >= 0) {
+                        buf[q] = h[kn * st];
+                        cb[q] = cpc[kn * (size_t)ncol];
+                    }
+                    x = (k == nz - 1) ? dk : dk - ck * x;
+                    h[k * st] = x * norm;
+                }
+            }
+        }
     }
 }
 
@@ -269,8 +304,8 @@ __global__ void __launch_bounds__(256) k_project(SlcParams P, const double *__re
         const double fx = t1[tx][r];
         const double fy = t0[tx][r + 1];
         const size_t I = i + 1, J = j + 1, K = k + 1;
-        u[I * usx + J * usy + K] -= dt * ((fx - f0) / P.dx);
-        v[I * vsx + J * vsy + K] -= dt * ((fy - f0) / P.dy);
+        u[I * usx + J * usy + K] -= dt * ((fx - f0) * P.inv_dx);
+        v[I * vsx + J * vsy + K] -= dt * ((fy - f0) * P.inv_dy);
         if (k < nz - 1) {
             const double fz = t0[tx + 1][r];
             w[I * wsx + J * wsy + K] -= dt * ((fz - f0) / dz_c[k + 1]);
@@ -293,22 +328,22 @@ __global__ void __launch_bounds__(256) k_bulk_partials(SlcParams P, double *__re
 {
     __shared__ double red[256];
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const long long n = (long long)nx * ny * nz;
+    const int ncol = nx * ny;
     const double c = c_dev ? *c_dev : 0.0;
     const size_t usx = (size_t)(ny + 2) * (nz + 2), usy = nz + 2;
     double acc = 0.0;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t % nz);
-        const long long q = t / nz;
-        const int j = (int)(q % ny), i = (int)(q / ny);
-        double *up = u + (size_t)(i + 1) * usx + (size_t)(j + 1) * usy + (k + 1);
-        double val = *up;
-        if (c_dev) {
-            val = val + c;
-            *up = val;
+    // block b owns columns b, b + gridDim.x, ...; its threads stride over k
+    for (int col = blockIdx.x; col < ncol; col += gridDim.x) {
+        const int i = col / ny, j = col - (col / ny) * ny;
+        double *up = u + (size_t)(i + 1) * usx + (size_t)(j + 1) * usy + 1;
+        for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+            double val = up[k];
+            if (c_dev) {
+                val = val + c;
+                up[k] = val;
+            }
+            acc = fma(val, __ldg(dz_f + k), acc);
         }
-        acc = fma(val, dz_f[k], acc);
     }
     red[threadIdx.x] = acc;
     __syncthreads();
@@ -386,10 +421,9 @@ cudaError_t launch_thomas_poisson(const SlcParams &P, double *hat, double *cp, c
                                   const double *ky2, const double *cl, const double *cr,
                                   cudaStream_t s)
 {
-    const long long ncol = (long long)P.nx * (P.ny / 2 + 1);
+    const long long nthr = 2LL * P.nx * (P.ny / 2 + 1);
     const double norm = 1.0 / ((double)P.nx * (double)P.ny);
-    k_thomas<<<(unsigned)((ncol + 255) / 256), 256, 0, s>>>(P, (double2 *)hat, cp, kx2, ky2, cl,
-                                                          cr, norm);
+    k_thomas<<<(unsigned)((nthr + 255) / 256), 256, 0, s>>>(P, hat, cp, kx2, ky2, cl, cr, norm);
     count_launches(1);
     return cudaGetLastError();
 }

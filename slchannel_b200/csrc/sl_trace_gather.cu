@@ -99,21 +99,22 @@ __device__ __forceinline__ double xy_diffusion(const SlcParams &P, const double 
 // MODE 0: one foot of depth dt on field fn (SLAdvector.advect).
 // MODE 1: BDF1 predictor ubar + dt R(fn)            (solver.py:760-771).
 // MODE 2: BDF2 predictor 4/3 ubar - 1/3 ubarbar + (2/3)dt Rh (solver.py:846-903).
+// Launch geometry of k_sl: a block is kTileK consecutive z arrival points
+// (one warp each 32) x kTileJ y-rows at one x index; grid (z tiles, y tiles, nx).
+constexpr int kTileK = 64, kTileJ = kThreads / kTileK;
+
 template <int C, int O, int MODE>
-__global__ void __launch_bounds__(kThreads) k_sl(SlcParams P, Vel3 M, const double *__restrict__ fn,
-                                                 const double *__restrict__ fnm1, double dt,
-                                                 double *__restrict__ out,
-                                                 unsigned long long *nclamp)
+__global__ void __launch_bounds__(kThreads, 2) k_sl(SlcParams P, Vel3 M, const double *__restrict__ fn,
+                                                    const double *__restrict__ fnm1, double dt,
+                                                    double *__restrict__ out,
+                                                    unsigned long long *nclamp)
 {
     const int nzi = (C == 2) ? P.nz - 1 : P.nz;
-    const long long n = (long long)P.nx * P.ny * nzi;
-    const long long p = (long long)blockIdx.x * kThreads + threadIdx.x;
+    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
+    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
+    const int i = blockIdx.z;
     unsigned ncl = 0;
-    if (p < n) {
-        const int k = (int)(p % nzi);
-        const long long q = p / nzi;
-        const int j = (int)(q % P.ny);
-        const int i = (int)(q / P.ny);
+    if (k < nzi && j < P.ny) {
         double xa, ya, za;
         arrival_point<C>(P, i, j, k, xa, ya, za);
         double us0, vs0, ws0;
@@ -219,13 +220,12 @@ template <int O, int MODE>
 void launch_sl_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
                  unsigned long long *ncl, cudaStream_t s)
 {
-    const long long nc = (long long)P.nx * P.ny * P.nz;
-    const long long nw = (long long)P.nx * P.ny * (P.nz - 1);
-    k_sl<0, O, MODE><<<blocks_for(nc), kThreads, 0, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl);
-    k_sl<1, O, MODE><<<blocks_for(nc), kThreads, 0, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl);
-    if (nw > 0)
-        k_sl<2, O, MODE><<<blocks_for(nw), kThreads, 0, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl);
-    count_launches(nw > 0 ? 3 : 2);
+    const dim3 gc((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
+    const dim3 gw((P.nz - 1 + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
+    k_sl<0, O, MODE><<<gc, kThreads, 0, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl);
+    k_sl<1, O, MODE><<<gc, kThreads, 0, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl);
+    if (P.nz > 1) k_sl<2, O, MODE><<<gw, kThreads, 0, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl);
+    count_launches(P.nz > 1 ? 3 : 2);
 }
 
 }  // namespace

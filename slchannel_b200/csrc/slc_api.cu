@@ -574,6 +574,8 @@ int slc_divergence_raw(int nx, int ny, int nz, double dx, double dy, const doubl
     P.nz = nz;
     P.dx = dx;
     P.dy = dy;
+    P.inv_dx = 1.0 / dx;
+    P.inv_dy = 1.0 / dy;
     SLC_CK(launch_divergence(P, Tri{u, v, w}, dz_f, div, S(stream)), "divergence");
     return SLC_OK;
 }

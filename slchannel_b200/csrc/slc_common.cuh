@@ -99,10 +99,15 @@ __device__ __forceinline__ int wrap_index(int i, int n)
 
 __device__ __forceinline__ int wrap_base(double f, int n)
 {
-    // f = floor(s) as a double; any magnitude (saturating conversion), NaN -> 0
-    long long i = (long long)f;
-    long long r = i % n;
-    return (int)(r < 0 ? r + n : r);
+    // f = floor(s), an integer-valued double.  Fast path: already in [0, n)
+    // (every foot within a period); otherwise reduce with floor division.
+    // NaN or huge values end in [0, n) too, so indices never leave the array.
+    const double dn = (double)n;
+    if (f >= 0.0 && f < dn) return (int)f;
+    double r = f - dn * floor(f / dn);
+    if (!(r >= 0.0)) r = 0.0;
+    if (r >= dn) r = dn - 1.0;
+    return (int)r;
 }
 
 // Continuous face index kf in [0, nz] of a physical z: analytic inverse of

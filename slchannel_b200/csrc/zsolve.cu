@@ -62,18 +62,25 @@ __global__ void k_zsolve_tables(SlcParams P, const double *dz_c, const double *d
     }
 }
 
+constexpr int kZWarps = 4;  // warps (columns) per block
+
+__host__ __device__ __forceinline__ int zpad(int k) { return k + (k >> 3); }  // bank skew, 1 per 8
+
 template <int CH>
-__global__ void __launch_bounds__(256) k_zsolve(SlcParams P, double *u, double *v, double *w,
-                                                const double *__restrict__ tab_uv,
-                                                const double *__restrict__ tab_w)
+__global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u, double *v,
+                                                         double *w,
+                                                         const double *__restrict__ tab_uv,
+                                                         const double *__restrict__ tab_w)
 {
-    const int lane = threadIdx.x & 31;
-    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    extern __shared__ double zsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long wid = (long long)blockIdx.x * kZWarps + wib;
     const long long ncol = (long long)P.nx * P.ny;
     if (wid >= 3 * ncol) return;  // whole warps exit together
+    double *sm = zsm + wib * zpad(32 * CH);
     const int comp = (int)(wid / ncol);
-    const long long col = wid % ncol;
-    const int i = (int)(col / P.ny), j = (int)(col % P.ny);
+    const int col = (int)(wid - (long long)comp * ncol);
+    const int i = col / P.ny, j = col - (col / P.ny) * P.ny;
     const GhostShape g = ghost_shape(comp, P.nx, P.ny, P.nz);
     double *base = comp == 0 ? u : (comp == 1 ? v : w);
     double *colp = base + (size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + 1;
@@ -81,10 +88,17 @@ __global__ void __launch_bounds__(256) k_zsolve(SlcParams P, double *u, double *
     const double *tab = comp == 2 ? tab_w : tab_uv;
     const double *al = tab, *inv = tab + n, *cp = tab + 2 * n;
 
+    // coalesced column load, transposed through shared memory into per-lane chunks
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+        const int k = q * 32 + lane;
+        if (k < n) sm[zpad(k)] = colp[k];
+    }
+    __syncwarp();
     const int s = lane * CH;
     double d[CH];
 #pragma unroll
-    for (int q = 0; q < CH; ++q) d[q] = (s + q < n) ? colp[s + q] : 0.0;
+    for (int q = 0; q < CH; ++q) d[q] = (s + q < n) ? sm[zpad(s + q)] : 0.0;
 
     // forward: chunk map y_out = A y_in + B
     double A = 1.0, B = 0.0;
@@ -148,9 +162,17 @@ __global__ void __launch_bounds__(256) k_zsolve(SlcParams P, double *u, double *
             d[q] = x;
         }
     }
+    // back through shared memory for a coalesced store
+    __syncwarp();
 #pragma unroll
     for (int q = 0; q < CH; ++q)
-        if (s + q < n) colp[s + q] = d[q];
+        if (s + q < n) sm[zpad(s + q)] = d[q];
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+        const int k = q * 32 + lane;
+        if (k < n) colp[k] = sm[zpad(k)];
+    }
 }
 
 }  // namespace
@@ -167,16 +189,20 @@ cudaError_t launch_zsolve(const SlcParams &P, TriMut f, const double *tab_uv, co
                           cudaStream_t s)
 {
     const long long warps = 3LL * P.nx * P.ny;
-    const unsigned blocks = (unsigned)((warps * 32 + 255) / 256);
+    const unsigned blocks = (unsigned)((warps + kZWarps - 1) / kZWarps);
     const int need = (P.nz + 31) / 32;  // chunk length per lane
-    if (need <= 1) k_zsolve<1><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
-    else if (need <= 2) k_zsolve<2><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
-    else if (need <= 4) k_zsolve<4><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
-    else if (need <= 8) k_zsolve<8><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
-    else if (need <= 12) k_zsolve<12><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
-    else if (need <= 16) k_zsolve<16><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
-    else if (need <= 32) k_zsolve<32><<<blocks, 256, 0, s>>>(P, f.u, f.v, f.w, tab_uv, tab_w);
+#define ZS(CHV)                                                                              \
+    k_zsolve<CHV><<<blocks, kZWarps * 32, kZWarps * zpad(32 * CHV) * sizeof(double), s>>>( \
+        P, f.u, f.v, f.w, tab_uv, tab_w)
+    if (need <= 1) ZS(1);
+    else if (need <= 2) ZS(2);
+    else if (need <= 4) ZS(4);
+    else if (need <= 8) ZS(8);
+    else if (need <= 12) ZS(12);
+    else if (need <= 16) ZS(16);
+    else if (need <= 32) ZS(32);
     else return cudaErrorInvalidValue;  // nz > 1024
+#undef ZS
     count_launches(1);
     return cudaGetLastError();
 }
