@@ -39,6 +39,7 @@ LX, LY, LZ = 4 * math.pi, 2 * math.pi, 2.0
 GAMMA = 2.0
 RE_B = 2792.8
 DT = 0.01
+MIXED_ERROR_STEPS = 20
 
 
 def parse_args():
@@ -51,6 +52,8 @@ def parse_args():
     ap.add_argument("--order", type=int, default=6)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--mixed-error-steps", type=int, default=20)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0,
                     help="CPU seconds the cpu_baseline sample aims for")
     return ap.parse_args()
@@ -366,6 +369,70 @@ def run_reference(args):
 # GPU arm
 # ---------------------------------------------------------------------------
 
+STATE = ("u", "v", "w", "u_nm1", "v_nm1", "w_nm1", "p")
+
+
+def copy_state(dst, src):
+    for name in STATE:
+        getattr(dst, name).copy_(getattr(src, name))
+    dst._dt_prev_step = src._dt_prev_step
+
+
+def measure_mixed(flow64, n, order, K, W, dist):
+    """The mixed-precision form on the same workload and state: device-timed
+    steps/s, and its velocity error against the FP64 form after a number of
+    free-running steps from a common state."""
+    import torch
+
+    from slchannel_b200.solver import SLChannelFlow
+    from slchannel_b200.utils import compute_divergence
+
+    flow32 = SLChannelFlow(config=config(n, order, "mixed"), allocate_fields=True)
+    flow32.set_state(flow64.u, flow64.v, flow64.w, flow64.p)
+    flow32.step_sl_bdf2(DT)  # allocates the history; then adopt the FP64 history
+    copy_state(flow32, flow64)
+    for _ in range(W):
+        flow32.step_sl_bdf2(DT)
+    flow32._grid.timing(True)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        flow32.step_sl_bdf2(DT)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    phases = flow32._grid.timing_read()
+    flow32._grid.timing(False)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    world = dist.get_world_size() if dist else 1
+    # error against the FP64 form from a common state
+    copy_state(flow32, flow64)
+    S = MIXED_ERROR_STEPS
+    errs = []
+    for _ in range(S):
+        flow64.step_sl_bdf2(DT)
+        flow32.step_sl_bdf2(DT)
+    for c in "uvw":
+        a, b = getattr(flow32, c), getattr(flow64, c)
+        scale = b.abs().max()
+        errs.append(((a - b).abs().max() / scale).item())
+    l2 = math.sqrt(sum(((getattr(flow32, c) - getattr(flow64, c)) ** 2).sum().item() for c in "uvw")
+                   / sum((getattr(flow64, c) ** 2).sum().item() for c in "uvw"))
+    div = compute_divergence(flow32.u, flow32.v, flow32.w, n, n, n, flow32.dx, flow32.dy, flow32.dz_f)
+    sl_ms, sl_cnt = phases["sl"]
+    return {"value": world * K / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / K,
+            "sl_kernel_ms_per_step": sl_ms / max(sl_cnt, 1),
+            "phase_ms": {p: v[0] / max(v[1], 1) for p, v in phases.items() if v[1]},
+            "vs_fp64_after_steps": S, "rel_linf_err_vs_fp64": max(errs), "rel_l2_err_vs_fp64": l2,
+            "max_div": float(div.abs().max()),
+            "form": "FP32 fluctuation about FP64 plane means in trace+gather; rest FP64"}
+
+
 def run_b200(args):
     import torch
 
@@ -470,6 +537,10 @@ def run_b200(args):
            "d2h_bytes_per_step": d2h, "steps": Ke, "ms_per_step": e2e_max / Ke,
            "path": "SLChannelFlow.step_sl_bdf2 with state in pinned host memory"}
 
+    mixed = None
+    if not args.no_mixed:
+        mixed = measure_mixed(flow, n, order, K, W, dist)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
@@ -481,6 +552,7 @@ def run_b200(args):
         "mpoint_updates_per_s": value * 3 * n**3 / 1e6,
         "phase_ms": phase_ms, "max_div": max_div,
         "gpu_launches": int(launches), "roofline": roofline, "clocks": clocks, "e2e": e2e,
+        "mixed": mixed,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_cpu, desc, threads = cpu_step_sample(n, order, args.cpu_budget_s)
@@ -495,7 +567,9 @@ def run_b200(args):
 
 
 def main():
+    global MIXED_ERROR_STEPS
     args = parse_args()
+    MIXED_ERROR_STEPS = args.mixed_error_steps
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -28,6 +28,9 @@ struct slc_grid {
     double *partials = nullptr, *scal = nullptr;
     unsigned long long *ncl_scratch = nullptr;
     double *mid[3] = {nullptr, nullptr, nullptr};
+    int mixed = 0;          // SLC_PREC_MIXED
+    bool mixed_ready = false;
+    MixedWS mws{};
     size_t ghost_elems[4] = {0, 0, 0, 0};
     cufftHandle fwd = 0, inv = 0;
     bool plans = false;
@@ -178,6 +181,25 @@ int ensure_mid(slc_grid *g)
     return SLC_OK;
 }
 
+int ensure_mixed(slc_grid *g)
+{
+    if (g->mixed_ready) return SLC_OK;
+    const SlcParams &P = g->P;
+    g->mws.nzp[0] = g->mws.nzp[1] = mixed_nzp(P.nz + 2);
+    g->mws.nzp[2] = mixed_nzp(P.nz + 1);
+    for (int q = 0; q < 9; ++q) {
+        const size_t n = (size_t)P.nx * P.ny * g->mws.nzp[q % 3];
+        int rc = dalloc(g, &g->mws.f32[q], n, "mixed FP32 node buffer");
+        if (rc) return rc;
+        rc = dalloc(g, &g->mws.mean[q], (size_t)P.nz + 2, "mixed plane mean");
+        if (rc) return rc;
+    }
+    int rc = dalloc(g, &g->mws.partials, mixed_partials_doubles(P), "mixed mean partials");
+    if (rc) return rc;
+    g->mixed_ready = true;
+    return SLC_OK;
+}
+
 unsigned long long *counter(slc_grid *g, int64_t *user)
 {
     return user ? (unsigned long long *)user : g->ncl_scratch;
@@ -223,6 +245,23 @@ int do_apply_bc(slc_grid *g, double *u, double *v, double *w, cudaStream_t s)
 int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *const prev[3],
                          double dt, double *const out[3], int64_t *nclamp, cudaStream_t s)
 {
+    if (g->mixed) {
+        int rc = ensure_mixed(g);
+        if (rc) return rc;
+        long t = tim_begin(g, SLC_PHASE_MID, s);
+        SLC_CK(launch_mixed_prepare(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
+                                    Tri{nullptr, nullptr, nullptr}, g->mws, s),
+               "mixed-form pack");
+        tim_end(g, t, s);
+        unsigned long long *ncl = counter(g, nclamp);
+        SLC_CK(cudaMemsetAsync(ncl, 0, sizeof(unsigned long long), s), "memset");
+        t = tim_begin(g, SLC_PHASE_SL, s);
+        SLC_CK(launch_sl_mixed(g->P, 2, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
+                               g->mws, dt, TriMut{out[0], out[1], out[2]}, ncl, s),
+               "mixed trace+gather BDF2");
+        tim_end(g, t, s);
+        return SLC_OK;
+    }
     int rc = ensure_mid(g);
     if (rc) return rc;
     long t = tim_begin(g, SLC_PHASE_MID, s);
@@ -293,6 +332,7 @@ int slc_grid_create(const slc_grid_desc *d, slc_grid **out)
     P.n_iters = d->n_traj_iters;
     P.top_neumann = d->top_wall_neumann ? 1 : 0;
     P.xy_lagged = d->xy_rhs_lagged ? 1 : 0;
+    g->mixed = d->precision == SLC_PREC_MIXED ? 1 : 0;
     g->Lx = d->Lx;
     g->Ly = d->Ly;
     P.dx = d->Lx / nx;
@@ -501,6 +541,19 @@ int slc_advect(slc_grid *g, const double *fu, const double *fv, const double *fw
     unsigned long long *ncl = counter(g, nclamp);
     cudaStream_t s = S(stream);
     SLC_CK(cudaMemsetAsync(ncl, 0, sizeof(unsigned long long), s), "memset");
+    if (g->mixed) {
+        int rc = ensure_mixed(g);
+        if (rc) return rc;
+        SLC_CK(launch_mixed_prepare(g->P, Tri{fu, fv, fw}, Tri{fu, fv, fw}, Tri{mid_u, mid_v, mid_w},
+                                    g->mws, s),
+               "mixed-form pack");
+        long t = tim_begin(g, SLC_PHASE_SL, s);
+        SLC_CK(launch_sl_mixed(g->P, 0, Tri{fu, fv, fw}, Tri{fu, fv, fw}, g->mws, dt,
+                               TriMut{ou, ov, ow}, ncl, s),
+               "mixed advect");
+        tim_end(g, t, s);
+        return SLC_OK;
+    }
     long t = tim_begin(g, SLC_PHASE_SL, s);
     SLC_CK(launch_sl(g->P, 0, Tri{fu, fv, fw}, Tri{fu, fv, fw}, Tri{mid_u, mid_v, mid_w}, false, dt,
                      TriMut{ou, ov, ow}, ncl, s),
@@ -638,9 +691,21 @@ int slc_step_bdf1(slc_grid *g, double *const cur[3], double *const next[3], doub
     unsigned long long *ncl = counter(g, nclamp);
     SLC_CK(cudaMemsetAsync(ncl, 0, sizeof(unsigned long long), s), "memset");
     Tri c3{cur[0], cur[1], cur[2]};
+    if (g->mixed) {
+        rc = ensure_mixed(g);
+        if (rc) return rc;
+        long tm = tim_begin(g, SLC_PHASE_MID, s);
+        SLC_CK(launch_mixed_prepare(g->P, c3, c3, Tri{nullptr, nullptr, nullptr}, g->mws, s),
+               "mixed-form pack");
+        tim_end(g, tm, s);
+    }
     long t = tim_begin(g, SLC_PHASE_SL, s);
-    SLC_CK(launch_sl(g->P, 1, c3, c3, c3, false, dt, TriMut{next[0], next[1], next[2]}, ncl, s),
-           "trace+gather BDF1");
+    if (g->mixed)
+        SLC_CK(launch_sl_mixed(g->P, 1, c3, c3, g->mws, dt, TriMut{next[0], next[1], next[2]}, ncl, s),
+               "mixed trace+gather BDF1");
+    else
+        SLC_CK(launch_sl(g->P, 1, c3, c3, c3, false, dt, TriMut{next[0], next[1], next[2]}, ncl, s),
+               "trace+gather BDF1");
     tim_end(g, t, s);
     rc = do_zsolve(g, next[0], next[1], next[2], dt, s);
     if (rc) return rc;

@@ -67,4 +67,22 @@ cudaError_t launch_bulk_finish(const SlcParams &P, const double *partials, doubl
                                double U_bulk, double dt, double *bulk_out, double *shift_out,
                                cudaStream_t s);
 
-constexpr int kBulkBlocks = 296;  // 2 x 148 SMs, fixed for a deterministic sum
+constexpr int kBulkBlocks = 296;
+
+// ---- sl_mixed.cu -------------------------------------------------------------
+// Workspace of the mixed form.  Slot q = comp + 3 * which, which = 0 the near
+// field (V^n), 1 the far field (V^{n-1}), 2 the trajectory velocity U*.
+struct MixedWS {
+    float *f32[9];    // FP32 fluctuation node buffers (nx, ny, nzp[comp])
+    double *mean[9];  // FP64 plane-mean profiles (nz+2 levels for u, v; nz+1 for w)
+    double *partials; // mixed_partials_doubles() scratch for the plane means
+    int nzp[3];       // padded node-buffer row length per component
+};
+int mixed_nzp(int NZ);
+size_t mixed_partials_doubles(const SlcParams &P);
+// Plane means + FP32 packs of A, B and U* (= M when M.u != NULL, else 2A - B).
+cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const MixedWS &ws,
+                                 cudaStream_t s);
+// mode 0 one foot of A, 1 BDF1 predictor, 2 BDF2 predictor; fn/fnm1 FP64 fields for R.
+cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, const MixedWS &ws,
+                            double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s);  // 2 x 148 SMs, fixed for a deterministic sum
