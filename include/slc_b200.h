@@ -133,6 +133,28 @@ SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *v
  * Replaces solve_implicit_diffusion_{u,v,w} (slchannel/operators.py:382-630). */
 SLC_API int slc_zsolve(slc_grid *g, double *u, double *v, double *w, double dt, void *stream);
 
+/* The implicit wall-normal diffusion of slc_zsolve, for callers that must
+ * not allocate device memory: no handle, no cudaMalloc/cudaFree, no
+ * allocating library call.  This has no counterpart in the reference.
+ * It is meant for host codes whose own memory manager owns the device (a
+ * pooled or budgeted allocator that a library cudaMalloc would bypass or
+ * fail against) and for tight time loops where cudaMalloc's implicit device
+ * synchronisation is not acceptable.  The caller passes the fields (solved in
+ * place on their interiors, ghost-shaped as everywhere in this header) and the
+ * grid spacings dz_c (nz+1) and dz_f (nz) as device arrays; nu is the
+ * kinematic viscosity, top_wall_neumann selects the free-slip top closure.
+ * The Thomas tables live in one fixed device array of 6 * 1024 doubles
+ * (48 KiB) that every GPU loading the library keeps until process exit, so
+ * nz > 1024 is rejected with SLC_E_INVALID.  The first call on a device looks
+ * up that array's address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls on a device share the array and each call
+ * rewrites it before reading it: calls that overlap on the GPU (different
+ * streams, no ordering between them) race on it.  Errors are reported
+ * through slc_last_error(NULL). */
+SLC_API int slc_zsolve_noalloc(int nx, int ny, int nz, double nu, int top_wall_neumann,
+                               const double *dz_c, const double *dz_f, double dt, double *u,
+                               double *v, double *w, void *stream);
+
 /* Divergence of the staggered field, interior-shaped (nx, ny, nz) output.
  * Replaces compute_divergence (slchannel/utils.py:166-180). */
 SLC_API int slc_divergence(slc_grid *g, const double *u, const double *v, const double *w, double *div,

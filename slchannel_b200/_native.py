@@ -78,6 +78,7 @@ SIGNATURES = {
     "slc_timing": ([_P, _I], _I),
     "slc_timing_read": ([_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_L)], _I),
     "slc_kernel_launches": ([], _L),
+    "slc_zsolve_noalloc": ([_I, _I, _I, _D, _I, _P, _P, _D, _P, _P, _P, _P], _I),
 }
 
 PHASES = ("bc", "mid", "sl", "zsolve", "project", "bulk")

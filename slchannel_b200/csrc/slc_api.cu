@@ -282,6 +282,13 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
 
 }  // namespace
 
+// Record the message of a failed handle-free call (read with slc_last_error(NULL)).
+int slc_report_error(int code, const char *msg)
+{
+    g_create_err = msg;
+    return code;
+}
+
 extern "C" {
 
 const char *slc_version(void) { return "slc_b200 0.1"; }

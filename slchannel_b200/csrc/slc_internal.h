@@ -69,6 +69,9 @@ cudaError_t launch_bulk_finish(const SlcParams &P, const double *partials, doubl
 
 constexpr int kBulkBlocks = 296;
 
+// Message of a failed handle-free call, for slc_last_error(NULL); returns code.
+int slc_report_error(int code, const char *msg);
+
 // ---- sl_mixed.cu -------------------------------------------------------------
 // Workspace of the mixed form.  Slot q = comp + 3 * which, which = 0 the near
 // field (V^n), 1 the far field (V^{n-1}), 2 the trajectory velocity U*.

@@ -11,6 +11,10 @@
 // affine maps, and a 5-step warp scan of the per-chunk maps hands each lane
 // its incoming value.  The reference solves the same systems with parallel
 // cyclic reduction (tridiag.py:36-61); the results agree to rounding.
+#include <mutex>
+#include <string>
+
+#include "../../include/slc_b200.h"
 #include "slc_internal.h"
 
 namespace {
@@ -205,4 +209,77 @@ cudaError_t launch_zsolve(const SlcParams &P, TriMut f, const double *tab_uv, co
 #undef ZS
     count_launches(1);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// slc_zsolve_noalloc: the same z-solve for callers that must not allocate
+// device memory.  Its only scratch, the Thomas factorisation tables (6 nz
+// doubles), lives in this fixed device array instead of a handle's workspace.
+// ---------------------------------------------------------------------------
+
+constexpr int kNoAllocMaxNz = 1024;  // 6 * 1024 doubles = 48 KiB per GPU
+static __device__ __align__(256) double g_zsolve_noalloc_tables[6 * kNoAllocMaxNz];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_tables[kMaxDevices] = {};
+
+// Device address of the table array on the current device; looked up once
+// per device (in host code the array's name is only a stand-in symbol).
+int noalloc_tables(double **out)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return slc_report_error(SLC_E_CUDA, (std::string("cudaGetDevice: ") + cudaGetErrorString(e)).c_str());
+    if (dev < 0 || dev >= kMaxDevices)
+        return slc_report_error(SLC_E_INVALID, "slc_zsolve_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_tables[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_zsolve_noalloc_tables);
+        if (e != cudaSuccess || !p)
+            return slc_report_error(SLC_E_CUDA, (std::string("cudaGetSymbolAddress: ") +
+                                                 cudaGetErrorString(e)).c_str());
+        g_noalloc_tables[dev] = (double *)p;
+    }
+    *out = g_noalloc_tables[dev];
+    return SLC_OK;
+}
+
+}  // namespace
+
+extern "C" int slc_zsolve_noalloc(int nx, int ny, int nz, double nu, int top_wall_neumann,
+                                  const double *dz_c, const double *dz_f, double dt, double *u,
+                                  double *v, double *w, void *stream)
+{
+    if (nx < 1 || ny < 1 || nz < 2)
+        return slc_report_error(SLC_E_INVALID, "slc_zsolve_noalloc: needs nx, ny >= 1 and nz >= 2");
+    if (nz > kNoAllocMaxNz)
+        return slc_report_error(SLC_E_INVALID,
+                                ("slc_zsolve_noalloc: nz = " + std::to_string(nz) +
+                                 " exceeds the fixed table size (nz <= " +
+                                 std::to_string(kNoAllocMaxNz) + ")").c_str());
+    if (!dz_c || !dz_f || !u || !v || !w)
+        return slc_report_error(SLC_E_INVALID, "slc_zsolve_noalloc: null pointer");
+    double *tab = nullptr;
+    int rc = noalloc_tables(&tab);
+    if (rc) return rc;
+    SlcParams P{};
+    P.nx = nx;
+    P.ny = ny;
+    P.nz = nz;
+    P.nu = nu;
+    P.top_neumann = top_wall_neumann ? 1 : 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    // every entry of the tables the solve reads is rewritten first, so nothing
+    // needs clearing between calls
+    cudaError_t e = launch_zsolve_tables(P, dz_c, dz_f, dt, tab, tab + 3 * nz, s);
+    if (e == cudaSuccess) e = launch_zsolve(P, TriMut{u, v, w}, tab, tab + 3 * nz, s);
+    if (e != cudaSuccess)
+        return slc_report_error(SLC_E_CUDA, (std::string("slc_zsolve_noalloc: ") +
+                                             cudaGetErrorString(e)).c_str());
+    return SLC_OK;
 }
