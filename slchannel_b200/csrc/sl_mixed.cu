@@ -31,10 +31,11 @@ __device__ __forceinline__ void sample3_m(const SlcParams &P, const Vel3M &M, do
                                           double z, double &us, double &vs, double &ws)
 {
     const double zc = clampz(P, z);
-    const int c = face_cell(P, zc);
-    us = trilinear_mixed<0>(P, M.u, x, y, zc, c);
-    vs = trilinear_mixed<1>(P, M.v, x, y, zc, c);
-    ws = trilinear_mixed<2>(P, M.w, x, y, zc, c);
+    TriShared t;
+    tri_shared(P, x, y, zc, face_cell(P, zc), t);
+    us = tri_sample_mixed(M.u, t.ia0, t.ia1, t.txa, t.jb0, t.jb1, t.tyb, t.kc, t.wc0, t.wc1);
+    vs = tri_sample_mixed(M.v, t.ib0, t.ib1, t.txb, t.ja0, t.ja1, t.tya, t.kc, t.wc0, t.wc1);
+    ws = tri_sample_mixed(M.w, t.ib0, t.ib1, t.txb, t.jb0, t.jb1, t.tyb, t.kf, t.wf0, t.wf1);
 }
 
 __device__ __forceinline__ void trace_foot_m(const SlcParams &P, const Vel3M &M, double xa,

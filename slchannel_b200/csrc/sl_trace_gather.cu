@@ -34,11 +34,12 @@ __device__ __forceinline__ void add_clamps(unsigned long long *counter, unsigned
 __device__ __forceinline__ void sample3(const SlcParams &P, const Vel3 &M, double x, double y,
                                         double z, double &us, double &vs, double &ws)
 {
-    double zc = clampz(P, z);
-    int c = face_cell(P, zc);
-    us = trilinear<0>(P, M.u, x, y, zc, c);
-    vs = trilinear<1>(P, M.v, x, y, zc, c);
-    ws = trilinear<2>(P, M.w, x, y, zc, c);
+    const double zc = clampz(P, z);
+    TriShared t;
+    tri_shared(P, x, y, zc, face_cell(P, zc), t);
+    us = tri_sample(M.u, t.ia0, t.ia1, t.txa, t.jb0, t.jb1, t.tyb, t.kc, t.wc0, t.wc1);
+    vs = tri_sample(M.v, t.ib0, t.ib1, t.txb, t.ja0, t.ja1, t.tya, t.kc, t.wc0, t.wc1);
+    ws = tri_sample(M.w, t.ib0, t.ib1, t.txb, t.jb0, t.jb1, t.tyb, t.kf, t.wf0, t.wf1);
 }
 
 // Iterated midpoint rule continued from the first-iteration sample

@@ -91,7 +91,14 @@ __host__ __device__ inline NodeView<T> node_view(const T *base, int NY, int NZ)
 
 __device__ __forceinline__ int wrap_index(int i, int n)
 {
-    // small offsets around an already wrapped base: at most a few corrections
+    // an already wrapped base in [0, n) plus an offset in [-3, 3]: one
+    // branch-free correction each way when n >= 4 (n is uniform, so the
+    // fallback loop for tiny periods costs no divergence)
+    if (n >= 4) {
+        i += (i < 0) ? n : 0;
+        i -= (i >= n) ? n : 0;
+        return i;
+    }
     while (i < 0) i += n;
     while (i >= n) i -= n;
     return i;
@@ -252,40 +259,71 @@ __device__ __forceinline__ A gather_sum(const T *__restrict__ F, const Stencil<O
     return acc;
 }
 
-// Trilinear (order 2) sample of one trajectory-velocity component at
-// (x, y, z) with z inside [z_lo, z_hi] and the face cell of z given
-// (semilag.py:512-528 with traj_order = 2).
-template <int C, typename T>
-__device__ __forceinline__ double trilinear(const SlcParams &P, NodeView<T> V, double x, double y,
-                                            double z, int c_face)
+// One trilinear sample of node view V from precomputed corner indices and
+// weights (x: i0, i1, tx; y: j0, j1, ty; z: k0, wz0, wz1).
+template <typename T>
+__device__ __forceinline__ double tri_sample(NodeView<T> V, int i0, int i1, double tx, int j0, int j1,
+                                             double ty, int k0, double wz0, double wz1)
 {
-    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
-    double s = x * P.inv_dx + Comp<C>::shift_x;
-    double f = floor(s);
-    double tx = s - f;
-    int i0 = wrap_base(f, P.nx);
-    int i1 = (i0 + 1 == P.nx) ? 0 : i0 + 1;
-    s = y * P.inv_dy + Comp<C>::shift_y;
-    f = floor(s);
-    double ty = s - f;
-    int j0 = wrap_base(f, P.ny);
-    int j1 = (j0 + 1 == P.ny) ? 0 : j0 + 1;
-    int m0 = locate_m0(P, Comp<C>::centers, c_face, z);
-    int k0 = min(max(m0, 0), NZ - 2);
-    const double *zn = Comp<C>::centers ? P.zc : P.zf;
-    const double *di = (Comp<C>::centers ? P.dinv_c[2] : P.dinv_f[2]) + 2 * k0;
-    double wz0 = (z - __ldg(zn + k0 + 1)) * __ldg(di);
-    double wz1 = (z - __ldg(zn + k0)) * __ldg(di + 1);
-    double wx0 = 1.0 - tx, wy0 = 1.0 - ty;
     const T *p00 = V.p + i0 * V.sx + j0 * V.sy + k0;
     const T *p01 = V.p + i0 * V.sx + j1 * V.sy + k0;
     const T *p10 = V.p + i1 * V.sx + j0 * V.sy + k0;
     const T *p11 = V.p + i1 * V.sx + j1 * V.sy + k0;
-    double a00 = wz0 * (double)__ldg(p00) + wz1 * (double)__ldg(p00 + 1);
-    double a01 = wz0 * (double)__ldg(p01) + wz1 * (double)__ldg(p01 + 1);
-    double a10 = wz0 * (double)__ldg(p10) + wz1 * (double)__ldg(p10 + 1);
-    double a11 = wz0 * (double)__ldg(p11) + wz1 * (double)__ldg(p11 + 1);
+    const double a00 = wz0 * (double)__ldg(p00) + wz1 * (double)__ldg(p00 + 1);
+    const double a01 = wz0 * (double)__ldg(p01) + wz1 * (double)__ldg(p01 + 1);
+    const double a10 = wz0 * (double)__ldg(p10) + wz1 * (double)__ldg(p10 + 1);
+    const double a11 = wz0 * (double)__ldg(p11) + wz1 * (double)__ldg(p11 + 1);
+    const double wx0 = 1.0 - tx, wy0 = 1.0 - ty;
     return wx0 * (wy0 * a00 + ty * a01) + tx * (wy0 * a10 + ty * a11);
+}
+
+// The pieces of the three trilinear stencils at one point that the staggered
+// components share (semilag.py:512-528 with traj_order = 2): x offsets with
+// shift 0 (u) and -1/2 (v, w), y offsets with shift 0 (v) and -1/2 (u, w),
+// z intervals on the centres (u, v) and on the faces (w).
+struct TriShared {
+    int ia0, ia1, ib0, ib1;  // x: shift 0 / -1/2
+    int ja0, ja1, jb0, jb1;  // y: shift 0 / -1/2
+    double txa, txb, tya, tyb;
+    int kc, kf;              // z interval bases: centres / faces
+    double wc0, wc1, wf0, wf1;
+};
+
+__device__ __forceinline__ void tri_shared(const SlcParams &P, double x, double y, double z,
+                                           int c_face, TriShared &t)
+{
+    double sa = x * P.inv_dx;
+    double f = floor(sa);
+    t.txa = sa - f;
+    t.ia0 = wrap_base(f, P.nx);
+    t.ia1 = (t.ia0 + 1 == P.nx) ? 0 : t.ia0 + 1;
+    double sb = sa - 0.5;
+    f = floor(sb);
+    t.txb = sb - f;
+    t.ib0 = wrap_base(f, P.nx);
+    t.ib1 = (t.ib0 + 1 == P.nx) ? 0 : t.ib0 + 1;
+    sa = y * P.inv_dy;
+    f = floor(sa);
+    t.tya = sa - f;
+    t.ja0 = wrap_base(f, P.ny);
+    t.ja1 = (t.ja0 + 1 == P.ny) ? 0 : t.ja0 + 1;
+    sb = sa - 0.5;
+    f = floor(sb);
+    t.tyb = sb - f;
+    t.jb0 = wrap_base(f, P.ny);
+    t.jb1 = (t.jb0 + 1 == P.ny) ? 0 : t.jb0 + 1;
+    // centres: interval m0 = c + (z >= zc[c+1]), clamped to [0, nz]; faces: c in [0, nz-1]
+    int kc = c_face + (z >= __ldg(P.zc + c_face + 1) ? 1 : 0);
+    kc = min(max(kc, 0), P.nz);
+    const int kf = min(max(c_face, 0), P.nz - 1);
+    t.kc = kc;
+    t.kf = kf;
+    const double *dc = P.dinv_c[2] + 2 * kc;
+    const double *df = P.dinv_f[2] + 2 * kf;
+    t.wc0 = (z - __ldg(P.zc + kc + 1)) * __ldg(dc);
+    t.wc1 = (z - __ldg(P.zc + kc)) * __ldg(dc + 1);
+    t.wf0 = (z - __ldg(P.zf + kf + 1)) * __ldg(df);
+    t.wf1 = (z - __ldg(P.zf + kf)) * __ldg(df + 1);
 }
 
 // Arrival point of flat interior index (i, j, k) of component C
@@ -329,42 +367,25 @@ struct MixedView {
     const double *mean;
 };
 
-template <int C>
-__device__ __forceinline__ double trilinear_mixed(const SlcParams &P, MixedView V, double x,
-                                                  double y, double z, int c_face)
+// Mixed-form trilinear sample from the shared stencil pieces: FP32
+// fluctuation, FP64 mean profile interpolated in z.
+__device__ __forceinline__ double tri_sample_mixed(MixedView V, int i0, int i1, double tx, int j0,
+                                                   int j1, double ty, int k0, double wz0, double wz1)
 {
-    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
-    double s = x * P.inv_dx + Comp<C>::shift_x;
-    double f = floor(s);
-    const double tx = s - f;
-    const int i0 = wrap_base(f, P.nx);
-    const int i1 = (i0 + 1 == P.nx) ? 0 : i0 + 1;
-    s = y * P.inv_dy + Comp<C>::shift_y;
-    f = floor(s);
-    const double ty = s - f;
-    const int j0 = wrap_base(f, P.ny);
-    const int j1 = (j0 + 1 == P.ny) ? 0 : j0 + 1;
-    const int m0 = locate_m0(P, Comp<C>::centers, c_face, z);
-    const int k0 = min(max(m0, 0), NZ - 2);
-    const double *zn = Comp<C>::centers ? P.zc : P.zf;
-    const double *di = (Comp<C>::centers ? P.dinv_c[2] : P.dinv_f[2]) + 2 * k0;
-    const double wz0 = (z - __ldg(zn + k0 + 1)) * __ldg(di);
-    const double wz1 = (z - __ldg(zn + k0)) * __ldg(di + 1);
-    const float fz0 = (float)wz0, fz1 = (float)wz1;
-    const float fx0 = (float)(1.0 - tx), fx1 = (float)tx;
-    const float fy0 = (float)(1.0 - ty), fy1 = (float)ty;
     const NodeView<float> F = V.f;
     const float *p00 = F.p + i0 * F.sx + j0 * F.sy + k0;
     const float *p01 = F.p + i0 * F.sx + j1 * F.sy + k0;
     const float *p10 = F.p + i1 * F.sx + j0 * F.sy + k0;
     const float *p11 = F.p + i1 * F.sx + j1 * F.sy + k0;
+    const float fz0 = (float)wz0, fz1 = (float)wz1;
+    const float fx1 = (float)tx, fx0 = (float)(1.0 - tx);
+    const float fy1 = (float)ty, fy0 = (float)(1.0 - ty);
     const float a00 = fz0 * __ldg(p00) + fz1 * __ldg(p00 + 1);
     const float a01 = fz0 * __ldg(p01) + fz1 * __ldg(p01 + 1);
     const float a10 = fz0 * __ldg(p10) + fz1 * __ldg(p10 + 1);
     const float a11 = fz0 * __ldg(p11) + fz1 * __ldg(p11 + 1);
     const float fl = fx0 * (fy0 * a00 + fy1 * a01) + fx1 * (fy0 * a10 + fy1 * a11);
-    const double mean = wz0 * __ldg(V.mean + k0) + wz1 * __ldg(V.mean + k0 + 1);
-    return (double)fl + mean;
+    return (double)fl + (wz0 * __ldg(V.mean + k0) + wz1 * __ldg(V.mean + k0 + 1));
 }
 
 template <int O>
