@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         double xa, ya, za;
         arrival_point<C>(P, i, j, k, xa, ya, za);
         double us0, vs0, ws0;
-        sample3_m(P, M, xa, ya, za, us0, vs0, ws0);
+        arrival_sample<C>(P, M, i, j, k, NodeValMixed(), us0, vs0, ws0);
         double xd, yd, zd;
         trace_foot_m(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd, yd, zd);
         const double ubar = gather_foot_m<C, O>(P, FA, xd, yd, zd, ncl);

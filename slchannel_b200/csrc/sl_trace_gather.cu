@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sl(SlcParams P, Vel3 M, const d
         double xa, ya, za;
         arrival_point<C>(P, i, j, k, xa, ya, za);
         double us0, vs0, ws0;
-        sample3(P, M, xa, ya, za, us0, vs0, ws0);
+        arrival_sample<C>(P, M, i, j, k, NodeValF64(), us0, vs0, ws0);
 
         const NodeView<double> Fn = ghost_view<double>(C, fn, P.nx, P.ny, P.nz);
         double xd, yd, zd;
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kThreads) k_departure(SlcParams P, Vel3 M, dou
     double xa, ya, za;
     arrival_point<C>(P, i, j, k, xa, ya, za);
     double us0, vs0, ws0;
-    sample3(P, M, xa, ya, za, us0, vs0, ws0);
+    arrival_sample<C>(P, M, i, j, k, NodeValF64(), us0, vs0, ws0);
     trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd[p], yd[p], zd[p]);
 }
 

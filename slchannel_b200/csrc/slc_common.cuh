@@ -326,6 +326,61 @@ __device__ __forceinline__ void tri_shared(const SlcParams &P, double x, double 
     t.wf1 = (z - __ldg(P.zf + kf)) * __ldg(df + 1);
 }
 
+// Node value accessor for the arrival-point sample below (FP64 node views).
+struct NodeValF64 {
+    __device__ __forceinline__ double operator()(NodeView<double> V, int I, int J, int K) const
+    {
+        return __ldg(V.p + I * V.sx + J * V.sy + K);
+    }
+};
+
+// The trajectory velocity at the arrival point of component C (the first
+// fixed-point iteration of semilag.py:542-549, which samples at x_m = x_a).
+// The arrival point is a node of its own component and a cell centre/face of
+// the others, so the trilinear weights are exact halves and node values
+// (z between faces or centres uses the actual node tables):
+//   u at (i+1, j+1/2, c_{k+1}), v at (i+1/2, j+1, c_{k+1}), w at (i+1/2, j+1/2, f_{k+1})
+// in units of (dx, dy) and node tables c = z_c, f = z_f.  The reference's
+// generic weights agree with these to round-off.
+template <int C, class V3, class Val>
+__device__ __forceinline__ void arrival_sample(const SlcParams &P, const V3 &M, int i, int j, int k,
+                                               Val val, double &us, double &vs, double &ws)
+{
+    const int ip = (i + 1 == P.nx) ? 0 : i + 1;
+    const int jp = (j + 1 == P.ny) ? 0 : j + 1;
+    if (C == 0) {
+        us = val(M.u, ip, j, k + 1);
+        vs = 0.25 * ((val(M.v, i, j, k + 1) + val(M.v, ip, j, k + 1)) +
+                     (val(M.v, i, jp, k + 1) + val(M.v, ip, jp, k + 1)));
+        const double z = __ldg(P.zc + k + 1);
+        const double *df = P.dinv_f[2] + 2 * k;  // face interval k
+        const double w0 = (z - __ldg(P.zf + k + 1)) * __ldg(df);
+        const double w1 = (z - __ldg(P.zf + k)) * __ldg(df + 1);
+        ws = 0.5 * ((w0 * val(M.w, i, j, k) + w1 * val(M.w, i, j, k + 1)) +
+                    (w0 * val(M.w, ip, j, k) + w1 * val(M.w, ip, j, k + 1)));
+    } else if (C == 1) {
+        us = 0.25 * ((val(M.u, i, j, k + 1) + val(M.u, ip, j, k + 1)) +
+                     (val(M.u, i, jp, k + 1) + val(M.u, ip, jp, k + 1)));
+        vs = val(M.v, i, jp, k + 1);
+        const double z = __ldg(P.zc + k + 1);
+        const double *df = P.dinv_f[2] + 2 * k;
+        const double w0 = (z - __ldg(P.zf + k + 1)) * __ldg(df);
+        const double w1 = (z - __ldg(P.zf + k)) * __ldg(df + 1);
+        ws = 0.5 * ((w0 * val(M.w, i, j, k) + w1 * val(M.w, i, j, k + 1)) +
+                    (w0 * val(M.w, i, jp, k) + w1 * val(M.w, i, jp, k + 1)));
+    } else {
+        const double z = __ldg(P.zf + k + 1);
+        const double *dc = P.dinv_c[2] + 2 * (k + 1);  // centre interval k+1
+        const double c0 = (z - __ldg(P.zc + k + 2)) * __ldg(dc);
+        const double c1 = (z - __ldg(P.zc + k + 1)) * __ldg(dc + 1);
+        us = 0.5 * ((c0 * val(M.u, i, j, k + 1) + c1 * val(M.u, i, j, k + 2)) +
+                    (c0 * val(M.u, ip, j, k + 1) + c1 * val(M.u, ip, j, k + 2)));
+        vs = 0.5 * ((c0 * val(M.v, i, j, k + 1) + c1 * val(M.v, i, j, k + 2)) +
+                    (c0 * val(M.v, i, jp, k + 1) + c1 * val(M.v, i, jp, k + 2)));
+        ws = val(M.w, i, j, k + 1);
+    }
+}
+
 // Arrival point of flat interior index (i, j, k) of component C
 // (semilag.py:292-307).
 template <int C>
@@ -387,6 +442,14 @@ __device__ __forceinline__ double tri_sample_mixed(MixedView V, int i0, int i1, 
     const float fl = fx0 * (fy0 * a00 + fy1 * a01) + fx1 * (fy0 * a10 + fy1 * a11);
     return (double)fl + (wz0 * __ldg(V.mean + k0) + wz1 * __ldg(V.mean + k0 + 1));
 }
+
+// Node value accessor of a mixed view: mean[K] + fluctuation.
+struct NodeValMixed {
+    __device__ __forceinline__ double operator()(MixedView V, int I, int J, int K) const
+    {
+        return (double)__ldg(V.f.p + I * V.f.sx + J * V.f.sy + K) + __ldg(V.mean + K);
+    }
+};
 
 template <int O>
 struct StencilM {
