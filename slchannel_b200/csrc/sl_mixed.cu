@@ -27,48 +27,227 @@ __device__ __forceinline__ void add_clamps(unsigned long long *counter, unsigned
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(counter, (unsigned long long)tot);
 }
 
-__device__ __forceinline__ void sample3_m(const SlcParams &P, const Vel3M &M, double x, double y,
-                                          double z, double &us, double &vs, double &ws)
-{
-    const double zc = clampz(P, z);
-    TriShared t;
-    tri_shared(P, x, y, zc, face_cell(P, zc), t);
-    us = tri_sample_mixed(M.u, t.ia0, t.ia1, t.txa, t.jb0, t.jb1, t.tyb, t.kc, t.wc0, t.wc1);
-    vs = tri_sample_mixed(M.v, t.ib0, t.ib1, t.txb, t.ja0, t.ja1, t.tya, t.kc, t.wc0, t.wc1);
-    ws = tri_sample_mixed(M.w, t.ib0, t.ib1, t.txb, t.jb0, t.jb1, t.tyb, t.kf, t.wf0, t.wf1);
-}
+// ---- FP32 characteristic trace -------------------------------------------
+// A trajectory point is its arrival point plus an FP32 displacement.  In
+// index space (s = x/dx + shift) the arrival point is an integer or a
+// half-integer for both shifts 0 and -1/2, kept as an exact int part and a
+// float fraction in {0, 1/2}; adding the (small) displacement to the
+// fraction keeps positions accurate to FP32 round-off of a few cells, not of
+// the domain.  z is an absolute FP32 coordinate (z in [0, Lz]).
+struct Arr32 {
+    int xa, xb, ya, yb;      // integer parts for shift 0 (a) and -1/2 (b)
+    float fxa, fxb, fya, fyb;
+    double za;               // arrival height (exact); z = za + dz, dz FP32
+    float dzlo, dzhi;        // clamp bounds z_lo - za, z_hi - za
+};
 
-__device__ __forceinline__ void trace_foot_m(const SlcParams &P, const Vel3M &M, double xa,
-                                             double ya, double za, double half_dt, double us0,
-                                             double vs0, double ws0, double &xd, double &yd,
-                                             double &zd)
+template <int C>
+__device__ __forceinline__ Arr32 arrival32(const SlcParams &P, int i, int j, int k)
 {
-    double xm = xa - half_dt * us0;
-    double ym = ya - half_dt * vs0;
-    double zm = clampz(P, za - half_dt * ws0);
-    for (int it = 1; it < P.n_iters; ++it) {
-        double us, vs, ws;
-        sample3_m(P, M, xm, ym, zm, us, vs, ws);
-        xm = xa - half_dt * us;
-        ym = ya - half_dt * vs;
-        zm = clampz(P, za - half_dt * ws);
+    Arr32 a;
+    if (C == 0) {  // u: x = (i+1) dx, y = (j+1/2) dy, z = z_c[k+1]
+        a.xa = i + 1; a.fxa = 0.f; a.xb = i; a.fxb = 0.5f;
+        a.ya = j; a.fya = 0.5f; a.yb = j; a.fyb = 0.f;
+        a.za = __ldg(P.zc + k + 1);
+    } else if (C == 1) {  // v: x = (i+1/2) dx, y = (j+1) dy, z = z_c[k+1]
+        a.xa = i; a.fxa = 0.5f; a.xb = i; a.fxb = 0.f;
+        a.ya = j + 1; a.fya = 0.f; a.yb = j; a.fyb = 0.5f;
+        a.za = __ldg(P.zc + k + 1);
+    } else {  // w: x = (i+1/2) dx, y = (j+1/2) dy, z = z_f[k+1]
+        a.xa = i; a.fxa = 0.5f; a.xb = i; a.fxb = 0.f;
+        a.ya = j; a.fya = 0.5f; a.yb = j; a.fyb = 0.f;
+        a.za = __ldg(P.zf + k + 1);
     }
-    xd = 2.0 * xm - xa;
-    yd = 2.0 * ym - ya;
-    zd = 2.0 * zm - za;
+    a.dzlo = (float)(P.z_lo - a.za);
+    a.dzhi = (float)(P.z_hi - a.za);
+    return a;
 }
 
-template <int C, int O>
-__device__ __forceinline__ double gather_foot_m(const SlcParams &P, MixedView F, double xd,
-                                                double yd, double zd, unsigned &ncl)
+__device__ __forceinline__ int wrap_int(int v, int n)
 {
-    if (zd < P.z_lo || zd > P.z_hi) ncl += 1;
-    const double z = clampz(P, zd);
-    const int c = face_cell(P, z);
-    StencilM<O> st;
-    build_stencil_mixed<C, O>(P, F.f.sx, F.f.sy, xd, yd, z, c, st);
-    return gather_mixed<O>(F, st);
+    if (v >= 0 && v < n) return v;
+    int r = v % n;
+    return r < 0 ? r + n : r;
 }
+
+// Cell base and fraction of index-space coordinate (ip + fr), any float fr
+// (NaN or huge displacements end inside the period).
+__device__ __forceinline__ void split32(int ip, float fr, int n, int &base, float &t)
+{
+    fr = fminf(fmaxf(fr, -1.0e6f), 1.0e6f);
+    const float fl = floorf(fr);
+    t = fr - fl;
+    base = wrap_int(ip + (int)fl, n);
+}
+
+// Height displacement clamped so that za + dz stays in [z_lo, z_hi].
+__device__ __forceinline__ float clampdz(const Arr32 &A, float dz)
+{
+    return dz < A.dzlo ? A.dzlo : (dz > A.dzhi ? A.dzhi : dz);
+}
+
+// FP32 face cell (analytic inverse tanh map, semilag.py:400-416).
+__device__ __forceinline__ int face_cell32(const SlcParams &P, float z)
+{
+    const float lim = 0.99999994f;
+    float kf;
+    if (P.symmetric) {
+        float arg = (z * (float)P.two_over_Lz - 1.0f) * (float)P.tanh_g;
+        arg = fminf(fmaxf(arg, -lim), lim);
+        kf = (atanhf(arg) * (float)P.inv_gamma + 1.0f) * (float)P.half_nz;
+    } else {
+        float arg = (1.0f - z * (float)P.inv_Lz) * (float)P.tanh_g;
+        arg = fminf(fmaxf(arg, -lim), lim);
+        kf = (1.0f - atanhf(arg) * (float)P.inv_gamma) * (float)P.nzd;
+    }
+    kf = fminf(fmaxf(floorf(kf), 0.0f), (float)(P.nz - 1));
+    return (int)kf;
+}
+
+__device__ __forceinline__ float tri32(MixedView V, int i0, int i1, float tx, int j0, int j1,
+                                       float ty, int k0, float wz0, float wz1)
+{
+    const NodeView<float> F = V.f;
+    const float *p00 = F.p + i0 * F.sx + j0 * F.sy + k0;
+    const float *p01 = F.p + i0 * F.sx + j1 * F.sy + k0;
+    const float *p10 = F.p + i1 * F.sx + j0 * F.sy + k0;
+    const float *p11 = F.p + i1 * F.sx + j1 * F.sy + k0;
+    const float a00 = wz0 * __ldg(p00) + wz1 * __ldg(p00 + 1);
+    const float a01 = wz0 * __ldg(p01) + wz1 * __ldg(p01 + 1);
+    const float a10 = wz0 * __ldg(p10) + wz1 * __ldg(p10 + 1);
+    const float a11 = wz0 * __ldg(p11) + wz1 * __ldg(p11 + 1);
+    const float fl = (1.f - tx) * ((1.f - ty) * a00 + ty * a01) + tx * ((1.f - ty) * a10 + ty * a11);
+    return fl + (wz0 * __ldg(V.mean32 + k0) + wz1 * __ldg(V.mean32 + k0 + 1));
+}
+
+// Trajectory velocity at arrival + (ddx, ddy) (index units) and height
+// za + dz.  Heights enter the weights as differences formed in FP64 (an FP32
+// absolute height near z = Lz would carry ~1e-7 absolute error, a sizeable
+// fraction of the near-wall spacing).
+__device__ __forceinline__ void sample3_32(const SlcParams &P, const Vel3M &M, const Arr32 &A,
+                                           float ddx, float ddy, float dz, float &us, float &vs,
+                                           float &ws)
+{
+    int ia0, ib0, ja0, jb0;
+    float txa, txb, tya, tyb;
+    split32(A.xa, A.fxa + ddx, P.nx, ia0, txa);
+    split32(A.xb, A.fxb + ddx, P.nx, ib0, txb);
+    split32(A.ya, A.fya + ddy, P.ny, ja0, tya);
+    split32(A.yb, A.fyb + ddy, P.ny, jb0, tyb);
+    const int ia1 = (ia0 + 1 == P.nx) ? 0 : ia0 + 1, ib1 = (ib0 + 1 == P.nx) ? 0 : ib0 + 1;
+    const int ja1 = (ja0 + 1 == P.ny) ? 0 : ja0 + 1, jb1 = (jb0 + 1 == P.ny) ? 0 : jb0 + 1;
+    const double z = A.za + (double)dz;
+    const int c = face_cell32(P, (float)z);
+    const int kc = min(max(c + (z >= __ldg(P.zc + c + 1) ? 1 : 0), 0), P.nz);
+    const int kf = min(max(c, 0), P.nz - 1);
+    const float *dc = P.dinv_c32[2] + 2 * kc;
+    const float *df = P.dinv_f32[2] + 2 * kf;
+    const float wc0 = (float)(z - __ldg(P.zc + kc + 1)) * __ldg(dc);
+    const float wc1 = (float)(z - __ldg(P.zc + kc)) * __ldg(dc + 1);
+    const float wf0 = (float)(z - __ldg(P.zf + kf + 1)) * __ldg(df);
+    const float wf1 = (float)(z - __ldg(P.zf + kf)) * __ldg(df + 1);
+    us = tri32(M.u, ia0, ia1, txa, jb0, jb1, tyb, kc, wc0, wc1);
+    vs = tri32(M.v, ib0, ib1, txb, ja0, ja1, tya, kc, wc0, wc1);
+    ws = tri32(M.w, ib0, ib1, txb, jb0, jb1, tyb, kf, wf0, wf1);
+}
+
+// Iterated midpoint rule (semilag.py:542-552) in FP32 displacements; returns
+// the foot as displacements from the arrival point (x, y in index units).
+__device__ __forceinline__ void trace_foot32(const SlcParams &P, const Vel3M &M, const Arr32 &A,
+                                             float hdt, float us0, float vs0, float ws0,
+                                             float &ddx, float &ddy, float &ddz)
+{
+    const float idx = (float)P.inv_dx, idy = (float)P.inv_dy;
+    float mx = -hdt * us0 * idx;
+    float my = -hdt * vs0 * idy;
+    float mz = clampdz(A, -hdt * ws0);
+    for (int it = 1; it < P.n_iters; ++it) {
+        float us, vs, ws;
+        sample3_32(P, M, A, mx, my, mz, us, vs, ws);
+        mx = -hdt * us * idx;
+        my = -hdt * vs * idy;
+        mz = clampdz(A, -hdt * ws);
+    }
+    ddx = 2.f * mx;
+    ddy = 2.f * my;
+    ddz = 2.f * mz;
+}
+
+// Clamp-and-count the foot and interpolate the mixed field F there: FP32
+// weights and accumulation for the fluctuation, the FP64 mean profile through
+// the (FP32) z weights.
+template <int C, int O>
+__device__ __forceinline__ double gather_foot32(const SlcParams &P, MixedView F, const Arr32 &A,
+                                                float ddx, float ddy, float ddz, unsigned &ncl)
+{
+    constexpr int h = O / 2 - 1;
+    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
+    if (ddz < A.dzlo || ddz > A.dzhi) ncl += 1;
+    const double z = A.za + (double)clampdz(A, ddz);
+    const int xi = (C == 0) ? A.xa : A.xb;
+    const float xf = (C == 0) ? A.fxa : A.fxb;
+    const int yi = (C == 1) ? A.ya : A.yb;
+    const float yf = (C == 1) ? A.fya : A.fyb;
+    int bx, by;
+    float tx, ty;
+    split32(xi, xf + ddx, P.nx, bx, tx);
+    split32(yi, yf + ddy, P.ny, by, ty);
+    StencilM<O> st;
+#pragma unroll
+    for (int m = 0; m < O; ++m) st.xoff[m] = wrap_index(bx + m - h, P.nx) * F.f.sx;
+#pragma unroll
+    for (int m = 0; m < O; ++m) st.yoff[m] = wrap_index(by + m - h, P.ny) * F.f.sy;
+    uniform_weights<O, float>(P, tx, st.wx);
+    uniform_weights<O, float>(P, ty, st.wy);
+    const int c = face_cell32(P, (float)z);
+    const int m0 = Comp<C>::centers ? c + (z >= __ldg(P.zc + c + 1) ? 1 : 0) : c;
+    const int k0 = min(max(m0 - h, 0), NZ - O);
+    st.k0 = k0;
+    // z - z_node from the FP64 node table: FP32-rounded nodes would break
+    // sum(weights) = 1 at the level of (round-off / spacing), biasing the
+    // interpolant in proportion to the field itself
+    {
+        const double *zn = Comp<C>::centers ? P.zc : P.zf;
+        const float *di = (Comp<C>::centers ? P.dinv_c32[O] : P.dinv_f32[O]) + k0 * O;
+        float d[O], pre[O];
+#pragma unroll
+        for (int l = 0; l < O; ++l) d[l] = (float)(z - __ldg(zn + k0 + l));
+        pre[0] = 1.f;
+#pragma unroll
+        for (int l = 1; l < O; ++l) pre[l] = pre[l - 1] * d[l - 1];
+        float suf = 1.f;
+#pragma unroll
+        for (int m = O - 1; m >= 0; --m) {
+            st.wz[m] = pre[m] * suf * __ldg(di + m);
+            suf = suf * d[m];
+        }
+    }
+    float acc = 0.f;
+#pragma unroll
+    for (int i = 0; i < O; ++i) {
+        float accy = 0.f;
+#pragma unroll
+        for (int j = 0; j < O; ++j) {
+            const float *row = F.f.p + st.xoff[i] + st.yoff[j] + k0;
+            float accz = 0.f;
+#pragma unroll
+            for (int k = 0; k < O; ++k) accz = fmaf(st.wz[k], __ldg(row + k), accz);
+            accy = fmaf(st.wy[j], accz, accy);
+        }
+        acc = fmaf(st.wx[i], accy, acc);
+    }
+    double mean = 0.0;
+#pragma unroll
+    for (int k = 0; k < O; ++k) mean = fma((double)st.wz[k], __ldg(F.mean + k0 + k), mean);
+    return (double)acc + mean;
+}
+
+struct NodeValMixed32 {
+    __device__ __forceinline__ double operator()(MixedView V, int I, int J, int K) const
+    {
+        return (double)(__ldg(V.f.p + I * V.f.sx + J * V.f.sy + K) + __ldg(V.mean32 + K));
+    }
+};
 
 template <int C>
 __device__ __forceinline__ double xy_diffusion64(const SlcParams &P, const double *__restrict__ f,
@@ -103,21 +282,21 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int i = blockIdx.z;
     unsigned ncl = 0;
     if (k < nzi && j < P.ny) {
-        double xa, ya, za;
-        arrival_point<C>(P, i, j, k, xa, ya, za);
-        double us0, vs0, ws0;
-        arrival_sample<C>(P, M, i, j, k, NodeValMixed(), us0, vs0, ws0);
-        double xd, yd, zd;
-        trace_foot_m(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd, yd, zd);
-        const double ubar = gather_foot_m<C, O>(P, FA, xd, yd, zd, ncl);
+        const Arr32 A = arrival32<C>(P, i, j, k);
+        double u0, v0, w0;
+        arrival_sample<C>(P, M, i, j, k, NodeValMixed32(), u0, v0, w0);
+        const float us0 = (float)u0, vs0 = (float)v0, ws0 = (float)w0;
+        float ddx, ddy, ddz;
+        trace_foot32(P, M, A, (float)(0.5 * dt), us0, vs0, ws0, ddx, ddy, ddz);
+        const double ubar = gather_foot32<C, O>(P, FA, A, ddx, ddy, ddz, ncl);
         double res;
         if (MODE == 0) {
             res = ubar;
         } else if (MODE == 1) {
             res = ubar + dt * xy_diffusion64<C>(P, fn, i, j, k);
         } else {
-            trace_foot_m(P, M, xa, ya, za, dt, us0, vs0, ws0, xd, yd, zd);
-            const double ubb = gather_foot_m<C, O>(P, FB, xd, yd, zd, ncl);
+            trace_foot32(P, M, A, (float)dt, us0, vs0, ws0, ddx, ddy, ddz);
+            const double ubb = gather_foot32<C, O>(P, FB, A, ddx, ddy, ddz, ncl);
             const double Rn = xy_diffusion64<C>(P, fn, i, j, k);
             const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion64<C>(P, fnm1, i, j, k);
             res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
@@ -171,6 +350,7 @@ __global__ void __launch_bounds__(256) k_plane_partials(SlcParams P, MeanSrcs S,
 // are 2 mean(A) - mean(B) instead of summed.
 struct MeanPtrs {
     double *m[9];
+    float *m32[9];
 };
 
 __global__ void k_plane_finish(SlcParams P, int nf, const double *partials, int ldp, int G,
@@ -195,6 +375,7 @@ __global__ void k_plane_finish(SlcParams P, int nf, const double *partials, int 
             m = s * inv;
         }
         out.m[f][k] = m;
+        out.m32[f][k] = (float)m;
     }
 }
 
@@ -244,6 +425,7 @@ MixedView mview(const MixedWS &ws, int slot, const SlcParams &P)
     const int comp = slot % 3;
     v.f = node_view<float>(ws.f32[slot], P.ny, ws.nzp[comp]);
     v.mean = ws.mean[slot];
+    v.mean32 = ws.mean32[slot];
     return v;
 }
 
@@ -283,7 +465,10 @@ cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const 
     const int ldp = P.nz + 2;
     k_plane_partials<<<dim3(kMeanBlocks, nf), 256, 0, s>>>(P, S, ws.partials, ldp);
     MeanPtrs mp;
-    for (int f = 0; f < 9; ++f) mp.m[f] = ws.mean[f];
+    for (int f = 0; f < 9; ++f) {
+        mp.m[f] = ws.mean[f];
+        mp.m32[f] = ws.mean32[f];
+    }
     k_plane_finish<<<9, 256, 0, s>>>(P, nf, ws.partials, ldp, kMeanBlocks, mp, explicit_m ? 0 : 1);
     PackArgs a{};
     for (int c = 0; c < 3; ++c) {

@@ -193,6 +193,8 @@ int ensure_mixed(slc_grid *g)
         if (rc) return rc;
         rc = dalloc(g, &g->mws.mean[q], (size_t)P.nz + 2, "mixed plane mean");
         if (rc) return rc;
+        rc = dalloc(g, &g->mws.mean32[q], (size_t)P.nz + 2, "mixed plane mean fp32");
+        if (rc) return rc;
     }
     int rc = dalloc(g, &g->mws.partials, mixed_partials_doubles(P), "mixed mean partials");
     if (rc) return rc;

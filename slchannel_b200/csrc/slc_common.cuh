@@ -412,100 +412,17 @@ __device__ __forceinline__ double clampz(const SlcParams &P, double z)
 
 // ---------------------------------------------------------------------------
 // Mixed form: a component stored as an FP32 node buffer of fluctuations about
-// an FP64 per-level (plane-mean) profile, value(i,j,k) = mean[k] + f[i,j,k].
-// Positions, stencil location and the z weights stay FP64; the fluctuation's
-// weights, loads and tensor-product accumulation are FP32; the mean profile
-// is interpolated in z in FP64 (the x,y weights sum to one).
+// an FP64 per-level (plane-mean) profile, value(i,j,k) = mean[k] + f[i,j,k]
+// (mean32: the profile rounded to FP32, for trajectory samples).
 // ---------------------------------------------------------------------------
 struct MixedView {
     NodeView<float> f;
     const double *mean;
-};
-
-// Mixed-form trilinear sample from the shared stencil pieces: FP32
-// fluctuation, FP64 mean profile interpolated in z.
-__device__ __forceinline__ double tri_sample_mixed(MixedView V, int i0, int i1, double tx, int j0,
-                                                   int j1, double ty, int k0, double wz0, double wz1)
-{
-    const NodeView<float> F = V.f;
-    const float *p00 = F.p + i0 * F.sx + j0 * F.sy + k0;
-    const float *p01 = F.p + i0 * F.sx + j1 * F.sy + k0;
-    const float *p10 = F.p + i1 * F.sx + j0 * F.sy + k0;
-    const float *p11 = F.p + i1 * F.sx + j1 * F.sy + k0;
-    const float fz0 = (float)wz0, fz1 = (float)wz1;
-    const float fx1 = (float)tx, fx0 = (float)(1.0 - tx);
-    const float fy1 = (float)ty, fy0 = (float)(1.0 - ty);
-    const float a00 = fz0 * __ldg(p00) + fz1 * __ldg(p00 + 1);
-    const float a01 = fz0 * __ldg(p01) + fz1 * __ldg(p01 + 1);
-    const float a10 = fz0 * __ldg(p10) + fz1 * __ldg(p10 + 1);
-    const float a11 = fz0 * __ldg(p11) + fz1 * __ldg(p11 + 1);
-    const float fl = fx0 * (fy0 * a00 + fy1 * a01) + fx1 * (fy0 * a10 + fy1 * a11);
-    return (double)fl + (wz0 * __ldg(V.mean + k0) + wz1 * __ldg(V.mean + k0 + 1));
-}
-
-// Node value accessor of a mixed view: mean[K] + fluctuation.
-struct NodeValMixed {
-    __device__ __forceinline__ double operator()(MixedView V, int I, int J, int K) const
-    {
-        return (double)__ldg(V.f.p + I * V.f.sx + J * V.f.sy + K) + __ldg(V.mean + K);
-    }
+    const float *mean32;
 };
 
 template <int O>
 struct StencilM {
     int xoff[O], yoff[O], k0;
     float wx[O], wy[O], wz[O];
-    double wz64[O];
 };
-
-template <int C, int O>
-__device__ __forceinline__ void build_stencil_mixed(const SlcParams &P, int sx, int sy, double x,
-                                                    double y, double z, int c_face, StencilM<O> &st)
-{
-    constexpr int h = O / 2 - 1;
-    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
-    double s = x * P.inv_dx + Comp<C>::shift_x;
-    double f = floor(s);
-    int b = wrap_base(f, P.nx);
-#pragma unroll
-    for (int m = 0; m < O; ++m) st.xoff[m] = wrap_index(b + m - h, P.nx) * sx;
-    uniform_weights<O, float>(P, (float)(s - f), st.wx);
-    s = y * P.inv_dy + Comp<C>::shift_y;
-    f = floor(s);
-    b = wrap_base(f, P.ny);
-#pragma unroll
-    for (int m = 0; m < O; ++m) st.yoff[m] = wrap_index(b + m - h, P.ny) * sy;
-    uniform_weights<O, float>(P, (float)(s - f), st.wy);
-    const int m0 = locate_m0(P, Comp<C>::centers, c_face, z);
-    const int k0 = min(max(m0 - h, 0), NZ - O);
-    st.k0 = k0;
-    const double *zn = Comp<C>::centers ? P.zc : P.zf;
-    const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
-    z_weights<O, double>(zn, dinv, k0, z, st.wz64);
-#pragma unroll
-    for (int m = 0; m < O; ++m) st.wz[m] = (float)st.wz64[m];
-}
-
-// FP32 order^3 contraction of the fluctuation plus the FP64 mean profile.
-template <int O>
-__device__ __forceinline__ double gather_mixed(MixedView V, const StencilM<O> &st)
-{
-    float acc = 0.f;
-#pragma unroll
-    for (int i = 0; i < O; ++i) {
-        float accy = 0.f;
-#pragma unroll
-        for (int j = 0; j < O; ++j) {
-            const float *row = V.f.p + st.xoff[i] + st.yoff[j] + st.k0;
-            float accz = 0.f;
-#pragma unroll
-            for (int k = 0; k < O; ++k) accz = fmaf(st.wz[k], __ldg(row + k), accz);
-            accy = fmaf(st.wy[j], accz, accy);
-        }
-        acc = fmaf(st.wx[i], accy, acc);
-    }
-    double mean = 0.0;
-#pragma unroll
-    for (int k = 0; k < O; ++k) mean = fma(st.wz64[k], __ldg(V.mean + st.k0 + k), mean);
-    return (double)acc + mean;
-}

@@ -78,6 +78,7 @@ int slc_report_error(int code, const char *msg);
 struct MixedWS {
     float *f32[9];    // FP32 fluctuation node buffers (nx, ny, nzp[comp])
     double *mean[9];  // FP64 plane-mean profiles (nz+2 levels for u, v; nz+1 for w)
+    float *mean32[9]; // the same profiles rounded to FP32 (trajectory samples)
     double *partials; // mixed_partials_doubles() scratch for the plane means
     int nzp[3];       // padded node-buffer row length per component
 };
