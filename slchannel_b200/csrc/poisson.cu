@@ -332,17 +332,37 @@ __global__ void __launch_bounds__(256) k_bulk_partials(SlcParams P, double *__re
     const double c = c_dev ? *c_dev : 0.0;
     const size_t usx = (size_t)(ny + 2) * (nz + 2), usy = nz + 2;
     double acc = 0.0;
-    // block b owns columns b, b + gridDim.x, ...; its threads stride over k
-    for (int col = blockIdx.x; col < ncol; col += gridDim.x) {
-        const int i = col / ny, j = col - (col / ny) * ny;
-        double *up = u + (size_t)(i + 1) * usx + (size_t)(j + 1) * usy + 1;
+    // block b owns columns b, b + G, b + 2G, ...; its threads stride over k.
+    // Four columns are loaded before they are accumulated (memory-level
+    // parallelism); the summation order is fixed, so the result is too.
+    const int G = gridDim.x;
+    for (int col0 = blockIdx.x; col0 < ncol; col0 += 4 * G) {
         for (int k = threadIdx.x; k < nz; k += blockDim.x) {
-            double val = up[k];
-            if (c_dev) {
-                val = val + c;
-                up[k] = val;
+            double val[4];
+            double *ptr[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int col = col0 + q * G;
+                ptr[q] = nullptr;
+                val[q] = 0.0;
+                if (col < ncol) {
+                    const int i = col / ny, j = col - (col / ny) * ny;
+                    ptr[q] = u + (size_t)(i + 1) * usx + (size_t)(j + 1) * usy + 1 + k;
+                    val[q] = *ptr[q];
+                }
             }
-            acc = fma(val, __ldg(dz_f + k), acc);
+            const double dz = __ldg(dz_f + k);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (ptr[q]) {
+                    double v = val[q];
+                    if (c_dev) {
+                        v = v + c;
+                        *ptr[q] = v;
+                    }
+                    acc = fma(v, dz, acc);
+                }
+            }
         }
     }
     red[threadIdx.x] = acc;

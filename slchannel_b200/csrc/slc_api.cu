@@ -133,7 +133,8 @@ int ensure_zsolve_tables(slc_grid *g, double dt, cudaStream_t s)
 {
     if (g->zs_valid && g->zs_dt == dt) return SLC_OK;
     const int nz = g->P.nz;
-    SLC_CK(launch_zsolve_tables(g->P, g->dzc, g->dzf, dt, g->zs_tab, g->zs_tab + 3 * nz, s),
+    SLC_CK(launch_zsolve_tables(g->P, g->dzc, g->dzf, dt, g->zs_tab,
+                                g->zs_tab + zsolve_table_doubles(nz) / 2, s),
            "z-solve tables");
     g->zs_dt = dt;
     g->zs_valid = true;
@@ -148,7 +149,9 @@ int do_zsolve(slc_grid *g, double *u, double *v, double *w, double dt, cudaStrea
     long t = tim_begin(g, SLC_PHASE_ZSOLVE, s);
     int rc = ensure_zsolve_tables(g, dt, s);
     if (rc) return rc;
-    SLC_CK(launch_zsolve(g->P, TriMut{u, v, w}, g->zs_tab, g->zs_tab + 3 * g->P.nz, s), "z-solve");
+    SLC_CK(launch_zsolve(g->P, TriMut{u, v, w}, g->zs_tab,
+                         g->zs_tab + zsolve_table_doubles(g->P.nz) / 2, s),
+           "z-solve");
     tim_end(g, t, s);
     return SLC_OK;
 }
@@ -452,7 +455,7 @@ int slc_grid_create(const slc_grid_desc *d, slc_grid **out)
     CREATE_CK(dalloc(g, &g->rhs, nreal, "Poisson rhs"));
     CREATE_CK(dalloc(g, &g->hat, 2 * ncplx, "Poisson spectrum"));
     CREATE_CK(dalloc(g, &g->cpw, ncplx, "Poisson Thomas scratch"));
-    CREATE_CK(dalloc(g, &g->zs_tab, (size_t)6 * nz, "z-solve tables"));
+    CREATE_CK(dalloc(g, &g->zs_tab, zsolve_table_doubles(nz), "z-solve tables"));
     CREATE_CK(dalloc(g, &g->partials, (size_t)kBulkBlocks, "bulk partials"));
     CREATE_CK(dalloc(g, &g->scal, (size_t)8, "scalars"));
     CREATE_CK(dalloc(g, &g->ncl_scratch, (size_t)1, "clamp counter"));

@@ -41,6 +41,17 @@ cudaError_t launch_lincomb(const double *a, const double *b, double ca, double c
 // ---- zsolve.cu ---------------------------------------------------------------
 // Thomas factorisation tables of (I - dt nu Dzz) with the wall closures:
 // tab_uv = [alpha(nz) | invden(nz) | cprime(nz)], tab_w likewise with nz-1.
+// Column chunk per lane of the z-solve (ceil(nz/32) rounded up to an
+// instantiated size) and the table layout: each of the six tables (alpha,
+// invden, c' for u/v, then for w) holds 32 * chunk entries, entry k at
+// (k % chunk) * 32 + k / chunk so that a warp's lanes read consecutive words.
+__host__ __device__ inline int zsolve_chunk(int nz)
+{
+    const int need = (nz + 31) / 32;
+    return need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : need <= 8 ? 8 : need <= 12 ? 12
+         : need <= 16 ? 16 : 32;
+}
+inline size_t zsolve_table_doubles(int nz) { return (size_t)6 * 32 * zsolve_chunk(nz); }
 cudaError_t launch_zsolve_tables(const SlcParams &P, const double *dz_c, const double *dz_f,
                                  double dt, double *tab_uv, double *tab_w, cudaStream_t s);
 cudaError_t launch_zsolve(const SlcParams &P, TriMut f, const double *tab_uv, const double *tab_w,
@@ -67,7 +78,7 @@ cudaError_t launch_bulk_finish(const SlcParams &P, const double *partials, doubl
                                double U_bulk, double dt, double *bulk_out, double *shift_out,
                                cudaStream_t s);
 
-constexpr int kBulkBlocks = 296;
+constexpr int kBulkBlocks = 1184;  // 8 x 148 SMs; fixed, so the sum order is too
 
 // Message of a failed handle-free call, for slc_last_error(NULL); returns code.
 int slc_report_error(int code, const char *msg);

@@ -29,9 +29,10 @@ __global__ void k_zsolve_tables(SlcParams P, const double *dz_c, const double *d
     const int nz = P.nz;
     const int n = which == 0 ? nz : nz - 1;
     if (n <= 0) return;
+    const int CH = zsolve_chunk(nz), L = 32 * CH;
     double *al = which == 0 ? tab_uv : tab_w;
-    double *inv = al + n;
-    double *cp = inv + n;
+    double *inv = al + L;
+    double *cp = inv + L;
     double cprev = 0.0;
     for (int k = 0; k < n; ++k) {
         double dl, dr, dc;
@@ -59,9 +60,10 @@ __global__ void k_zsolve_tables(SlcParams P, const double *dz_c, const double *d
         const double denom = b - a * cprev;
         const double id = 1.0 / denom;
         const double cpk = c * id;
-        al[k] = -a * id;
-        inv[k] = id;
-        cp[k] = cpk;
+        const int pos = (k % CH) * 32 + k / CH;  // lane-interleaved
+        al[pos] = -a * id;
+        inv[pos] = id;
+        cp[pos] = cpk;
         cprev = cpk;
     }
 }
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u,
     double *colp = base + (size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + 1;
     const int n = comp == 2 ? P.nz - 1 : P.nz;
     const double *tab = comp == 2 ? tab_w : tab_uv;
-    const double *al = tab, *inv = tab + n, *cp = tab + 2 * n;
+    const double *al = tab, *inv = tab + 32 * CH, *cp = tab + 64 * CH;
 
     // coalesced column load, transposed through shared memory into per-lane chunks
 #pragma unroll
@@ -110,8 +112,8 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u,
     for (int q = 0; q < CH; ++q) {
         const int k = s + q;
         if (k < n) {
-            const double a = __ldg(al + k);
-            B = fma(a, B, __ldg(inv + k) * d[q]);
+            const double a = __ldg(al + q * 32 + lane);
+            B = fma(a, B, __ldg(inv + q * 32 + lane) * d[q]);
             A = a * A;
         }
     }
@@ -130,7 +132,7 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u,
     for (int q = 0; q < CH; ++q) {
         const int k = s + q;
         if (k < n) {
-            y = fma(__ldg(al + k), y, __ldg(inv + k) * d[q]);
+            y = fma(__ldg(al + q * 32 + lane), y, __ldg(inv + q * 32 + lane) * d[q]);
             d[q] = y;
         }
     }
@@ -142,7 +144,7 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u,
     for (int q = CH - 1; q >= 0; --q) {
         const int k = s + q;
         if (k < n) {
-            const double gk = -__ldg(cp + k);
+            const double gk = -__ldg(cp + q * 32 + lane);
             B = fma(gk, B, d[q]);
             A = gk * A;
         }
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u,
     for (int q = CH - 1; q >= 0; --q) {
         const int k = s + q;
         if (k < n) {
-            x = fma(-__ldg(cp + k), x, d[q]);
+            x = fma(-__ldg(cp + q * 32 + lane), x, d[q]);
             d[q] = x;
         }
     }
@@ -194,18 +196,18 @@ cudaError_t launch_zsolve(const SlcParams &P, TriMut f, const double *tab_uv, co
 {
     const long long warps = 3LL * P.nx * P.ny;
     const unsigned blocks = (unsigned)((warps + kZWarps - 1) / kZWarps);
-    const int need = (P.nz + 31) / 32;  // chunk length per lane
+    const int CH = zsolve_chunk(P.nz);  // chunk length per lane
 #define ZS(CHV)                                                                              \
     k_zsolve<CHV><<<blocks, kZWarps * 32, kZWarps * zpad(32 * CHV) * sizeof(double), s>>>( \
         P, f.u, f.v, f.w, tab_uv, tab_w)
-    if (need <= 1) ZS(1);
-    else if (need <= 2) ZS(2);
-    else if (need <= 4) ZS(4);
-    else if (need <= 8) ZS(8);
-    else if (need <= 12) ZS(12);
-    else if (need <= 16) ZS(16);
-    else if (need <= 32) ZS(32);
-    else return cudaErrorInvalidValue;  // nz > 1024
+    if (P.nz > 1024) return cudaErrorInvalidValue;
+    if (CH == 1) ZS(1);
+    else if (CH == 2) ZS(2);
+    else if (CH == 4) ZS(4);
+    else if (CH == 8) ZS(8);
+    else if (CH == 12) ZS(12);
+    else if (CH == 16) ZS(16);
+    else ZS(32);
 #undef ZS
     count_launches(1);
     return cudaGetLastError();
@@ -276,8 +278,9 @@ extern "C" int slc_zsolve_noalloc(int nx, int ny, int nz, double nu, int top_wal
     cudaStream_t s = (cudaStream_t)stream;
     // every entry of the tables the solve reads is rewritten first, so nothing
     // needs clearing between calls
-    cudaError_t e = launch_zsolve_tables(P, dz_c, dz_f, dt, tab, tab + 3 * nz, s);
-    if (e == cudaSuccess) e = launch_zsolve(P, TriMut{u, v, w}, tab, tab + 3 * nz, s);
+    const size_t half = zsolve_table_doubles(nz) / 2;  // <= 3 * 1024 for nz <= 1024
+    cudaError_t e = launch_zsolve_tables(P, dz_c, dz_f, dt, tab, tab + half, s);
+    if (e == cudaSuccess) e = launch_zsolve(P, TriMut{u, v, w}, tab, tab + half, s);
     if (e != cudaSuccess)
         return slc_report_error(SLC_E_CUDA, (std::string("slc_zsolve_noalloc: ") +
                                              cudaGetErrorString(e)).c_str());
