@@ -238,6 +238,65 @@ SLC_API int slc_timing_read(slc_grid *g, double *ms, int64_t *count);
  * own kernels; cuFFT's are not counted). */
 SLC_API int64_t slc_kernel_launches(void);
 
+/* ---- Ensembles of independent channels --------------------------------------
+ * No counterpart in the reference, which advances one channel per process.
+ * An ensemble advances n channels of uneven grids, viscosities and time steps
+ * together.  Every substep of the BDF2 step is one launch over all of them:
+ *  - the trace+gather is a persistent kernel over an (instance, component,
+ *    tile) work queue;
+ *  - the Poisson FFTs are one cuFFT call per group of instances sharing
+ *    (nx, ny);
+ *  - the step can be captured once per phase into a CUDA graph.
+ * Per instance the arithmetic is that of slc_step_bdf2 followed by
+ * slc_bulk_shift, so an instance matches the same channel stepped alone.
+ * FP64 form only. */
+typedef struct slc_ensemble slc_ensemble; /* opaque */
+
+/* n instances; descs[i] as for slc_grid_create (one order, one device,
+ * precision SLC_PREC_FP64, nz >= 2).  Synchronous. */
+SLC_API int slc_ensemble_create(const slc_grid_desc *descs, int n, slc_ensemble **out);
+SLC_API int slc_ensemble_destroy(slc_ensemble *e);
+SLC_API int slc_ensemble_size(const slc_ensemble *e);
+/* The instance's own handle (BDF1 bootstrap, diagnostics); owned by e. */
+SLC_API slc_grid *slc_ensemble_grid(slc_ensemble *e, int i);
+SLC_API const char *slc_ensemble_last_error(const slc_ensemble *e);
+
+/* Bind the caller's device fields and per-instance parameters:
+ *  - lev[(i * 3 + level) * 3 + comp]: three time levels of (u, v, w) per
+ *    instance, ghost-shaped;
+ *  - p[i]: the pressure;
+ *  - dt[i], U_bulk[i]: HOST arrays;
+ *  - nclamp: n device int64 clamp counters, or NULL;
+ *  - bulk_out: 2 n device doubles, [u_bulk, forcing] per instance.
+ * The step of phase ph reads V^{n-1} from level ph % 3 and V^n from level
+ * (ph + 1) % 3, and writes V^{n+1} into level (ph + 2) % 3.  Allocates the
+ * group FFT pools, plans and z-solve tables.  Drops captured graphs.
+ * Synchronous. */
+SLC_API int slc_ensemble_bind(slc_ensemble *e, double *const *lev, double *const *p,
+                              const double *dt, const double *U_bulk, int64_t *nclamp,
+                              double *bulk_out);
+
+/* Per-instance SL tile shape: 2^tkl[i] z points x 2^(8 - tkl[i]) y rows,
+ * tkl in [3, 8].  Results do not depend on it. */
+SLC_API int slc_ensemble_set_tiles(slc_ensemble *e, const int *tkl);
+SLC_API int slc_ensemble_get_tiles(const slc_ensemble *e, int *tkl);
+
+/* Tile-shape autotuner.  For each distinct grid shape it times the
+ * trace+gather of that shape's instances with z tiles of 32, 64 and 128
+ * points (`reps` launches each, after one warm-up) and keeps the fastest.
+ * Runs the phase's U* and trace+gather, so it overwrites the V^{n+1} level
+ * and the clamp counters.  tkl_out (n) and timings_ms (3 n) may be NULL.
+ * Synchronous. */
+SLC_API int slc_ensemble_autotune(slc_ensemble *e, int phase, int reps, int *tkl_out,
+                                  double *timings_ms, void *stream);
+
+/* One SL-BDF2 step of every instance, bulk shift included, in phase
+ * `phase` (0, 1, 2).  With use_graph, the first call per phase captures the
+ * step into a CUDA graph on a private stream; every call then launches it
+ * on `stream`.  The first call per phase must therefore not itself be under
+ * stream capture. */
+SLC_API int slc_ensemble_step_bdf2(slc_ensemble *e, int phase, int use_graph, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,6 +79,17 @@ SIGNATURES = {
     "slc_timing_read": ([_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_L)], _I),
     "slc_kernel_launches": ([], _L),
     "slc_zsolve_noalloc": ([_I, _I, _I, _D, _I, _P, _P, _D, _P, _P, _P, _P], _I),
+    "slc_ensemble_create": ([ctypes.POINTER(GridDesc), _I, ctypes.POINTER(_P)], _I),
+    "slc_ensemble_destroy": ([_P], _I),
+    "slc_ensemble_size": ([_P], _I),
+    "slc_ensemble_grid": ([_P, _I], _P),
+    "slc_ensemble_last_error": ([_P], ctypes.c_char_p),
+    "slc_ensemble_bind": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_D),
+                           ctypes.POINTER(_D), _P, _P], _I),
+    "slc_ensemble_set_tiles": ([_P, ctypes.POINTER(_I)], _I),
+    "slc_ensemble_get_tiles": ([_P, ctypes.POINTER(_I)], _I),
+    "slc_ensemble_autotune": ([_P, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_D), _P], _I),
+    "slc_ensemble_step_bdf2": ([_P, _I, _I, _P], _I),
 }
 
 PHASES = ("bc", "mid", "sl", "zsolve", "project", "bulk")

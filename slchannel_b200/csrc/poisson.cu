@@ -133,14 +133,14 @@ __device__ __forceinline__ double div_at(const SlcParams &P, const double *__res
 }
 
 // rhs[k][i][j] = div(i, j, k) / dt_div, through a shared-memory transpose.
-__global__ void __launch_bounds__(256) k_div_pack(SlcParams P, const double *__restrict__ u,
-                                                  const double *__restrict__ v,
-                                                  const double *__restrict__ w,
-                                                  const double *__restrict__ dz_f, double dt_div,
-                                                  double *__restrict__ rhs)
+__device__ __forceinline__ void div_pack_tile(const SlcParams &P, const double *__restrict__ u,
+                                              const double *__restrict__ v,
+                                              const double *__restrict__ w,
+                                              const double *__restrict__ dz_f, double dt_div,
+                                              double *__restrict__ rhs, int bx, int by, int bz)
 {
     __shared__ double tile[32][33];
-    const int i = blockIdx.z, j0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int i = bz, j0 = by * 32, k0 = bx * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += 8) {
         const int j = j0 + r, k = k0 + tx;
@@ -153,6 +153,15 @@ __global__ void __launch_bounds__(256) k_div_pack(SlcParams P, const double *__r
         const int k = k0 + r, j = j0 + tx;
         if (k < P.nz && j < P.ny) rhs[((size_t)k * P.nx + i) * P.ny + j] = tile[tx][r];
     }
+}
+
+__global__ void __launch_bounds__(256) k_div_pack(SlcParams P, const double *__restrict__ u,
+                                                  const double *__restrict__ v,
+                                                  const double *__restrict__ w,
+                                                  const double *__restrict__ dz_f, double dt_div,
+                                                  double *__restrict__ rhs)
+{
+    div_pack_tile(P, u, v, w, dz_f, dt_div, rhs, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 __global__ void k_divergence(SlcParams P, const double *__restrict__ u,
@@ -179,12 +188,12 @@ __global__ void k_divergence(SlcParams P, const double *__restrict__ u,
 
 constexpr int kPre = 8;  // loads kept in flight per thread in the sweeps
 
-__global__ void __launch_bounds__(256) k_thomas(SlcParams P, double *__restrict__ hat,
-                                                double *__restrict__ cpw,
-                                                const double *__restrict__ kx2,
-                                                const double *__restrict__ ky2,
-                                                const double *__restrict__ cl,
-                                                const double *__restrict__ cr, double norm)
+__device__ __forceinline__ void thomas_column(const SlcParams &P, double *__restrict__ hat,
+                                              double *__restrict__ cpw,
+                                              const double *__restrict__ kx2,
+                                              const double *__restrict__ ky2,
+                                              const double *__restrict__ cl,
+                                              const double *__restrict__ cr, double norm, int t)
 {
     // thread t handles part (t & 1) (0 real, 1 imaginary) of column t >> 1; the
     // coefficients are real, so the two parts are independent systems.  The
@@ -192,7 +201,6 @@ __global__ void __launch_bounds__(256) k_thomas(SlcParams P, double *__restrict_
     // a warp barrier.
     const int nky = P.ny / 2 + 1;
     const int ncol = P.nx * nky;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int col = t >> 1, part = t & 1;
     const bool active = col < ncol;
     const int nz = P.nz;
@@ -264,21 +272,32 @@ __global__ void __launch_bounds__(256) k_thomas(SlcParams P, double *__restrict_
     }
 }
 
+__global__ void __launch_bounds__(256) k_thomas(SlcParams P, double *__restrict__ hat,
+                                                double *__restrict__ cpw,
+                                                const double *__restrict__ kx2,
+                                                const double *__restrict__ ky2,
+                                                const double *__restrict__ cl,
+                                                const double *__restrict__ cr, double norm)
+{
+    thomas_column(P, hat, cpw, kx2, ky2, cl, cr, norm, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // --------------------------------------------------------------------------
 // Projection (projection.py:250-272): u -= dt dphi/dx, v -= dt dphi/dy,
 // w -= dt dphi/dz on the interiors, p interior <- phi.  phi is z-major; a tile
 // (i fixed, 33 j x 33 k, plus the x+1 plane) goes through shared memory.
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) k_project(SlcParams P, const double *__restrict__ phi,
-                                                 double *__restrict__ u, double *__restrict__ v,
-                                                 double *__restrict__ w, double *__restrict__ p,
-                                                 const double *__restrict__ dz_c, double dt)
+__device__ __forceinline__ void project_tile(const SlcParams &P, const double *__restrict__ phi,
+                                             double *__restrict__ u, double *__restrict__ v,
+                                             double *__restrict__ w, double *__restrict__ p,
+                                             const double *__restrict__ dz_c, double dt, int bx,
+                                             int by, int bz)
 {
     __shared__ double t0[33][33];  // [k][j], plane i
     __shared__ double t1[32][33];  // [k][j], plane i+1 (periodic)
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const int i = blockIdx.z, j0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int i = bz, j0 = by * 32, k0 = bx * 32;
     const int i1 = (i + 1 == nx) ? 0 : i + 1;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 33; r += 8) {
@@ -314,6 +333,14 @@ __global__ void __launch_bounds__(256) k_project(SlcParams P, const double *__re
     }
 }
 
+__global__ void __launch_bounds__(256) k_project(SlcParams P, const double *__restrict__ phi,
+                                                 double *__restrict__ u, double *__restrict__ v,
+                                                 double *__restrict__ w, double *__restrict__ p,
+                                                 const double *__restrict__ dz_c, double dt)
+{
+    project_tile(P, phi, u, v, w, p, dz_c, dt, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // --------------------------------------------------------------------------
 // Bulk velocity (utils.py:147-163): sum u dx dy dz_f / (Lx Ly Lz), summed in a
 // fixed order (fixed grid, fixed block tree, fixed finish) so reruns agree
@@ -321,10 +348,10 @@ __global__ void __launch_bounds__(256) k_project(SlcParams P, const double *__re
 // first and the sum taken over the shifted field.
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) k_bulk_partials(SlcParams P, double *__restrict__ u,
-                                                       const double *__restrict__ dz_f,
-                                                       const double *__restrict__ c_dev,
-                                                       double *__restrict__ partials)
+__device__ __forceinline__ void bulk_partial(const SlcParams &P, double *__restrict__ u,
+                                             const double *__restrict__ dz_f,
+                                             const double *__restrict__ c_dev,
+                                             double *__restrict__ partials, int bx, int G)
 {
     __shared__ double red[256];
     const int nx = P.nx, ny = P.ny, nz = P.nz;
@@ -335,8 +362,7 @@ __global__ void __launch_bounds__(256) k_bulk_partials(SlcParams P, double *__re
     // block b owns columns b, b + G, b + 2G, ...; its threads stride over k.
     // Four columns are loaded before they are accumulated (memory-level
     // parallelism); the summation order is fixed, so the result is too.
-    const int G = gridDim.x;
-    for (int col0 = blockIdx.x; col0 < ncol; col0 += 4 * G) {
+    for (int col0 = bx; col0 < ncol; col0 += 4 * G) {
         for (int k = threadIdx.x; k < nz; k += blockDim.x) {
             double val[4];
             double *ptr[4];
@@ -371,11 +397,20 @@ __global__ void __launch_bounds__(256) k_bulk_partials(SlcParams P, double *__re
         if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+    if (threadIdx.x == 0) partials[bx] = red[0];
 }
 
-__global__ void k_bulk_finish(const double *__restrict__ partials, int nparts, double dxdy_over_V,
-                              double U_bulk, double dt, double *bulk_out, double *shift_out)
+__global__ void __launch_bounds__(256) k_bulk_partials(SlcParams P, double *__restrict__ u,
+                                                       const double *__restrict__ dz_f,
+                                                       const double *__restrict__ c_dev,
+                                                       double *__restrict__ partials)
+{
+    bulk_partial(P, u, dz_f, c_dev, partials, blockIdx.x, gridDim.x);
+}
+
+__device__ __forceinline__ void bulk_finish(const double *__restrict__ partials, int nparts,
+                                            double dxdy_over_V, double U_bulk, double dt,
+                                            double *bulk_out, double *shift_out)
 {
     __shared__ double red[256];
     double acc = 0.0;
@@ -394,6 +429,84 @@ __global__ void k_bulk_finish(const double *__restrict__ partials, int nparts, d
             shift_out[0] = corr;
             shift_out[1] = corr / dt;
         }
+    }
+}
+
+__global__ void k_bulk_finish(const double *__restrict__ partials, int nparts, double dxdy_over_V,
+                              double U_bulk, double dt, double *bulk_out, double *shift_out)
+{
+    bulk_finish(partials, nparts, dxdy_over_V, U_bulk, dt, bulk_out, shift_out);
+}
+
+// ---- ensemble forms: one block per item, the instance's own arithmetic ----
+
+__global__ void k_bc_ens(const EnsInst *__restrict__ ins, const EnsItem *__restrict__ items,
+                         int lvl, int with_p)
+{
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    const SlcParams &P = I.P;
+    long long n[4];
+    for (int c = 0; c < 4; ++c) {
+        const BcCounts b = bc_counts(c, P.nx, P.ny, P.nz);
+        n[c] = (c < 3 || with_p) ? b.a + b.b + b.c : 0;
+    }
+    const long long t0 = (long long)it.a * blockDim.x + threadIdx.x;
+    for (long long t = t0; t < n[0] + n[1] + n[2] + n[3]; t += (long long)it.b * blockDim.x) {
+        if (t < n[0]) bc_one(P, 0, I.lev[lvl][0], t);
+        else if (t < n[0] + n[1]) bc_one(P, 1, I.lev[lvl][1], t - n[0]);
+        else if (t < n[0] + n[1] + n[2]) bc_one(P, 2, I.lev[lvl][2], t - n[0] - n[1]);
+        else bc_one(P, 3, I.p, t - n[0] - n[1] - n[2]);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_div_pack_ens(const EnsInst *__restrict__ ins,
+                                                      const EnsItem *__restrict__ items, int lvl)
+{
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    div_pack_tile(I.P, I.lev[lvl][0], I.lev[lvl][1], I.lev[lvl][2], I.dzf, (2.0 / 3.0) * I.dt,
+                  I.rhs, it.a, it.b, it.c);
+}
+
+__global__ void __launch_bounds__(256) k_thomas_ens(const EnsInst *__restrict__ ins,
+                                                    const EnsItem *__restrict__ items)
+{
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    const double norm = 1.0 / ((double)I.P.nx * (double)I.P.ny);
+    thomas_column(I.P, I.hat, I.cpw, I.kx2, I.ky2, I.cl, I.cr, norm,
+                  it.a * blockDim.x + threadIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_project_ens(const EnsInst *__restrict__ ins,
+                                                     const EnsItem *__restrict__ items, int lvl)
+{
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    project_tile(I.P, I.rhs, I.lev[lvl][0], I.lev[lvl][1], I.lev[lvl][2], I.p, I.dzc,
+                 (2.0 / 3.0) * I.dt, it.a, it.b, it.c);
+}
+
+__global__ void __launch_bounds__(256) k_bulk_partials_ens(const EnsInst *__restrict__ ins,
+                                                           const EnsItem *__restrict__ items,
+                                                           int lvl, int with_shift)
+{
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    bulk_partial(I.P, I.lev[lvl][0], I.dzf, with_shift ? I.scal : nullptr, I.partials, it.a,
+                 kBulkBlocks);
+}
+
+__global__ void k_bulk_finish_ens(const EnsInst *__restrict__ ins, int mode)
+{
+    const EnsInst &I = ins[blockIdx.x];
+    const double dxdy_over_V = (I.P.dx * I.P.dy) / (I.Lx * I.Ly * I.P.Lz);
+    if (mode == 0) {
+        bulk_finish(I.partials, kBulkBlocks, dxdy_over_V, I.U_bulk, I.dt, nullptr, I.scal);
+    } else {
+        bulk_finish(I.partials, kBulkBlocks, dxdy_over_V, 0.0, 1.0, I.bulk_out, nullptr);
+        if (threadIdx.x == 0) I.bulk_out[1] = I.scal[1];
     }
 }
 
@@ -472,6 +585,58 @@ cudaError_t launch_bulk_finish(const SlcParams &P, const double *partials, doubl
     const double dxdy_over_V = (P.dx * P.dy) / (Lx * Ly * P.Lz);
     k_bulk_finish<<<1, 256, 0, s>>>(partials, kBulkBlocks, dxdy_over_V, U_bulk, dt, bulk_out,
                                     shift_out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bc_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                          int with_p, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_bc_ens<<<nitems, 256, 0, s>>>(ins, items, lvl, with_p);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_div_pack_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                                cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_div_pack_ens<<<nitems, dim3(32, 8), 0, s>>>(ins, items, lvl);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_thomas_ens(const EnsInst *ins, const EnsItem *items, int nitems, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_thomas_ens<<<nitems, 256, 0, s>>>(ins, items);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                               cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_project_ens<<<nitems, dim3(32, 8), 0, s>>>(ins, items, lvl);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bulk_partials_ens(const EnsInst *ins, const EnsItem *items, int nitems,
+                                     int lvl, int with_shift, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_bulk_partials_ens<<<nitems, 256, 0, s>>>(ins, items, lvl, with_shift);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bulk_finish_ens(const EnsInst *ins, int ninst, int mode, cudaStream_t s)
+{
+    if (ninst <= 0) return cudaSuccess;
+    k_bulk_finish_ens<<<ninst, 256, 0, s>>>(ins, mode);
     count_launches(1);
     return cudaGetLastError();
 }

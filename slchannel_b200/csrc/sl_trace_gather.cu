@@ -104,17 +104,17 @@ __device__ __forceinline__ double xy_diffusion(const SlcParams &P, const double 
 // (one warp each 32) x kTileJ y-rows at one x index; grid (z tiles, y tiles, nx).
 constexpr int kTileK = 64, kTileJ = kThreads / kTileK;
 
+// One arrival point (i, j, k) of component C; out-of-range points only
+// contribute nothing.  Shared by the single-grid kernel below and the
+// persistent ensemble kernel, so both do the same arithmetic per point.
 template <int C, int O, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) k_sl(SlcParams P, Vel3 M, const double *__restrict__ fn,
-                                                    const double *__restrict__ fnm1, double dt,
-                                                    double *__restrict__ out,
-                                                    unsigned long long *nclamp)
+__device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
+                                         const double *__restrict__ fn,
+                                         const double *__restrict__ fnm1, double dt,
+                                         double *__restrict__ out, int i, int j, int k,
+                                         unsigned &ncl)
 {
     const int nzi = (C == 2) ? P.nz - 1 : P.nz;
-    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
-    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
-    const int i = blockIdx.z;
-    unsigned ncl = 0;
     if (k < nzi && j < P.ny) {
         double xa, ya, za;
         arrival_point<C>(P, i, j, k, xa, ya, za);
@@ -142,6 +142,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_sl(SlcParams P, Vel3 M, const d
         const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
         out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
     }
+}
+
+template <int C, int O, int MODE>
+__global__ void __launch_bounds__(kThreads, 2) k_sl(SlcParams P, Vel3 M, const double *__restrict__ fn,
+                                                    const double *__restrict__ fnm1, double dt,
+                                                    double *__restrict__ out,
+                                                    unsigned long long *nclamp)
+{
+    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
+    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
+    const int i = blockIdx.z;
+    unsigned ncl = 0;
+    sl_point<C, O, MODE>(P, M, fn, fnm1, dt, out, i, j, k, ncl);
     add_clamps(nclamp, ncl);
 }
 
@@ -215,6 +228,71 @@ Vel3 make_vel(const SlcParams &P, Tri mid, bool node)
         M.w = ghost_view<double>(2, mid.w, P.nx, P.ny, P.nz);
     }
     return M;
+}
+
+// Persistent BDF2 trace+gather over an ensemble's queue of (instance,
+// component, x index, tile) items.  The grid is sized to the resident limit;
+// each block takes the next item from an atomic counter, prefetched while it
+// works on the current one.  The instance's SlcParams are copied to shared
+// memory when the block moves to another instance.  Per point the arithmetic
+// is sl_point's, so an instance's result does not depend on the tile shape
+// or on the other instances.
+template <int O>
+__global__ void __launch_bounds__(kThreads, 2) k_sl_ens(const EnsInst *__restrict__ ins,
+                                                        const EnsItem *__restrict__ items,
+                                                        int nitems, int ph, unsigned *queue)
+{
+    __shared__ SlcParams sP;
+    __shared__ int s_item;
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+    int have = -1;
+    for (;;) {
+        __syncthreads();  // the previous item is done everywhere; s_item is published
+        const int it = s_item;
+        if (it >= nitems) break;
+        const EnsItem w = items[it];
+        if (w.inst != have) {
+            const unsigned long long *src = (const unsigned long long *)&ins[w.inst].P;
+            unsigned long long *dst = (unsigned long long *)&sP;
+            for (int q = threadIdx.x; q < (int)(sizeof(SlcParams) / 8); q += kThreads) dst[q] = src[q];
+            have = w.inst;
+        }
+        __syncthreads();  // sP ready; every thread has read s_item
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+        const EnsInst &I = ins[w.inst];
+        const int tkl = I.tkl;
+        const int k = ((w.c & 0xffff) << tkl) + (threadIdx.x & ((1 << tkl) - 1));
+        const int j = ((w.c >> 16) << (8 - tkl)) + (threadIdx.x >> tkl);
+        const int i = w.b;
+        Vel3 M;
+        M.u = ghost_view<double>(0, I.mid[0], sP.nx, sP.ny, sP.nz);
+        M.v = ghost_view<double>(1, I.mid[1], sP.nx, sP.ny, sP.nz);
+        M.w = ghost_view<double>(2, I.mid[2], sP.nx, sP.ny, sP.nz);
+        const double *fn = I.lev[ens_cur(ph)][w.a];
+        const double *fnm1 = I.lev[ens_prev(ph)][w.a];
+        double *out = I.lev[ens_next(ph)][w.a];
+        unsigned ncl = 0;
+        if (w.a == 0) sl_point<0, O, 2>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else if (w.a == 1) sl_point<1, O, 2>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else sl_point<2, O, 2>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
+        add_clamps(I.ncl, ncl);
+    }
+}
+
+__global__ void k_lincomb_ens(const EnsInst *__restrict__ ins, const EnsItem *__restrict__ items,
+                              int ph, double ca, double cb)
+{
+    const EnsItem w = items[blockIdx.x];
+    const EnsInst &I = ins[w.inst];
+    const GhostShape g = ghost_shape(w.a, I.P.nx, I.P.ny, I.P.nz);
+    const long long n = (long long)g.X * g.Y * g.Z;
+    const double *a = I.lev[ens_cur(ph)][w.a], *b = I.lev[ens_prev(ph)][w.a];
+    double *o = I.mid[w.a];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const long long p = (long long)w.b * 1024 + q * 256 + threadIdx.x;
+        if (p < n) o[p] = ca * a[p] + cb * b[p];
+    }
 }
 
 template <int O, int MODE>
@@ -303,6 +381,37 @@ cudaError_t launch_lincomb(const double *a, const double *b, double ca, double c
     unsigned blocks = blocks_for(n);
     if (blocks > 148 * 16) blocks = 148 * 16;
     k_lincomb<<<blocks, kThreads, 0, s>>>(a, b, ca, cb, out, n);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+int sl_ens_blocks_per_sm()
+{
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sl_ens<6>, kThreads, 0) != cudaSuccess)
+        return 1;
+    int nb4 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb4, k_sl_ens<4>, kThreads, 0) != cudaSuccess)
+        return 1;
+    const int m = nb < nb4 ? nb : nb4;
+    return m > 0 ? m : 1;
+}
+
+cudaError_t launch_sl_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
+                          unsigned *queue, int grid, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    if (order == 4) k_sl_ens<4><<<grid, kThreads, 0, s>>>(ins, items, nitems, ph, queue);
+    else k_sl_ens<6><<<grid, kThreads, 0, s>>>(ins, items, nitems, ph, queue);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lincomb_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph,
+                               cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_lincomb_ens<<<nitems, 256, 0, s>>>(ins, items, ph, 2.0, -1.0);
     count_launches(1);
     return cudaGetLastError();
 }

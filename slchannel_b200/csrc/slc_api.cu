@@ -10,38 +10,7 @@
 #include <vector>
 
 #include "../../include/slc_b200.h"
-#include "slc_internal.h"
-
-struct slc_grid {
-    SlcParams P{};
-    int device = 0;
-    double Lx = 0, Ly = 0;
-    double *zc = nullptr, *zf = nullptr, *dzc = nullptr, *dzf = nullptr;
-    double *dinv_c[SLC_MAX_ORDER + 1] = {}, *dinv_f[SLC_MAX_ORDER + 1] = {};
-    float *zc32 = nullptr, *zf32 = nullptr;
-    float *dinv_c32[SLC_MAX_ORDER + 1] = {}, *dinv_f32[SLC_MAX_ORDER + 1] = {};
-    double *kx2 = nullptr, *ky2 = nullptr, *cl = nullptr, *cr = nullptr;
-    double *rhs = nullptr, *hat = nullptr, *cpw = nullptr;
-    double *zs_tab = nullptr;
-    double zs_dt = 0.0;
-    bool zs_valid = false;
-    double *partials = nullptr, *scal = nullptr;
-    unsigned long long *ncl_scratch = nullptr;
-    double *mid[3] = {nullptr, nullptr, nullptr};
-    int mixed = 0;          // SLC_PREC_MIXED
-    bool mixed_ready = false;
-    MixedWS mws{};
-    size_t ghost_elems[4] = {0, 0, 0, 0};
-    cufftHandle fwd = 0, inv = 0;
-    bool plans = false;
-    std::vector<void *> allocs;
-    std::string err;
-    // per-phase event timing (slc_timing)
-    bool timing = false;
-    std::vector<cudaEvent_t> evs;  // pairs: [2i] start, [2i+1] end
-    std::vector<int> ev_phase;
-    size_t ev_used = 0;
-};
+#include "slc_grid.h"
 
 std::atomic<long long> g_slc_launches{0};
 

@@ -40,7 +40,7 @@ cudaError_t launch_lincomb(const double *a, const double *b, double ca, double c
 
 // ---- zsolve.cu ---------------------------------------------------------------
 // Thomas factorisation tables of (I - dt nu Dzz) with the wall closures:
-// tab_uv = [alpha(nz) | invden(nz) | cprime(nz)], tab_w likewise with nz-1.
+// tab_uv = [alpha | invden | cprime] for u and v, tab_w likewise for w (nz-1 rows).
 // Column chunk per lane of the z-solve (ceil(nz/32) rounded up to an
 // instantiated size) and the table layout: each of the six tables (alpha,
 // invden, c' for u/v, then for w) holds 32 * chunk entries, entry k at
@@ -100,4 +100,56 @@ cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const 
                                  cudaStream_t s);
 // mode 0 one foot of A, 1 BDF1 predictor, 2 BDF2 predictor; fn/fnm1 FP64 fields for R.
 cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, const MixedWS &ws,
-                            double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s);  // 2 x 148 SMs, fixed for a deterministic sum
+                            double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s);
+
+// ---- ensemble kernels (many independent channels, one launch per substep) ----
+// One channel as the multi-instance kernels see it.  The three time levels of
+// (u, v, w) are cycled by the step phase ph: V^{n-1} = lev[ph % 3],
+// V^n = lev[(ph + 1) % 3], V^{n+1} = lev[(ph + 2) % 3].
+struct EnsInst {
+    SlcParams P;
+    double *lev[3][3];
+    double *p;
+    double *mid[3];                 // U* = 2 V^n - V^{n-1}, ghost-shaped
+    const double *dzf, *dzc, *kx2, *ky2, *cl, *cr;
+    double *rhs, *hat, *cpw;        // Poisson workspaces (rhs, hat inside a group's FFT pools)
+    const double *zs_uv, *zs_w;     // z-solve tables at dt_eff = 2 dt / 3
+    double *partials, *scal;        // kBulkBlocks partial sums; [shift, forcing]
+    unsigned long long *ncl;        // departure-clamp counter
+    double *bulk_out;               // [u_bulk after the shift, forcing]
+    double dt, Lx, Ly, U_bulk;
+    int tkl;                        // SL tile: 2^tkl z points x 2^(8 - tkl) y rows
+};
+// A block's work: instance and three kernel-specific coordinates.
+struct EnsItem {
+    int inst, a, b, c;
+};
+__host__ __device__ inline int ens_prev(int ph) { return ph % 3; }
+__host__ __device__ inline int ens_cur(int ph) { return (ph + 1) % 3; }
+__host__ __device__ inline int ens_next(int ph) { return (ph + 2) % 3; }
+
+// sl_trace_gather.cu: persistent BDF2 trace+gather over the queue `items`
+// (inst, comp, i, tile index); `queue` is a zeroed counter.
+cudaError_t launch_sl_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
+                          unsigned *queue, int grid, cudaStream_t s);
+int sl_ens_blocks_per_sm();
+// U* for every instance: items (inst, comp, chunk of 1024 elements).
+cudaError_t launch_lincomb_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph,
+                               cudaStream_t s);
+// zsolve.cu: items (inst, block of kZWarps columns); chunk sizes up to max_ch.
+cudaError_t launch_zsolve_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                              int max_ch, cudaStream_t s);
+int zsolve_ens_warps();
+// poisson.cu
+cudaError_t launch_bc_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                          int with_p, cudaStream_t s);
+cudaError_t launch_div_pack_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                                cudaStream_t s);
+cudaError_t launch_thomas_ens(const EnsInst *ins, const EnsItem *items, int nitems,
+                              cudaStream_t s);
+cudaError_t launch_project_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                               cudaStream_t s);
+cudaError_t launch_bulk_partials_ens(const EnsInst *ins, const EnsItem *items, int nitems,
+                                     int lvl, int with_shift, cudaStream_t s);
+// mode 0: scal = [U_bulk - bulk, (U_bulk - bulk) / dt]; mode 1: bulk_out = [bulk, scal[1]].
+cudaError_t launch_bulk_finish_ens(const EnsInst *ins, int ninst, int mode, cudaStream_t s);

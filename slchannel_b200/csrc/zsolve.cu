@@ -72,18 +72,17 @@ constexpr int kZWarps = 4;  // warps (columns) per block
 
 __host__ __device__ __forceinline__ int zpad(int k) { return k + (k >> 3); }  // bank skew, 1 per 8
 
+// Column `wid` (component-major over the 3 nx ny columns) solved by the
+// calling warp, with `sm` its zpad(32 CH) doubles of shared memory.
 template <int CH>
-__global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u, double *v,
-                                                         double *w,
-                                                         const double *__restrict__ tab_uv,
-                                                         const double *__restrict__ tab_w)
+__device__ __forceinline__ void zsolve_warp(const SlcParams &P, double *u, double *v, double *w,
+                                            const double *__restrict__ tab_uv,
+                                            const double *__restrict__ tab_w, long long wid,
+                                            double *sm)
 {
-    extern __shared__ double zsm[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const long long wid = (long long)blockIdx.x * kZWarps + wib;
+    const int lane = threadIdx.x & 31;
     const long long ncol = (long long)P.nx * P.ny;
     if (wid >= 3 * ncol) return;  // whole warps exit together
-    double *sm = zsm + wib * zpad(32 * CH);
     const int comp = (int)(wid / ncol);
     const int col = (int)(wid - (long long)comp * ncol);
     const int i = col / P.ny, j = col - (col / P.ny) * P.ny;
@@ -178,6 +177,43 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u,
     for (int q = 0; q < CH; ++q) {
         const int k = q * 32 + lane;
         if (k < n) colp[k] = sm[zpad(k)];
+    }
+}
+
+template <int CH>
+__global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u, double *v,
+                                                         double *w,
+                                                         const double *__restrict__ tab_uv,
+                                                         const double *__restrict__ tab_w)
+{
+    extern __shared__ double zsm[];
+    const int wib = threadIdx.x >> 5;
+    zsolve_warp<CH>(P, u, v, w, tab_uv, tab_w, (long long)blockIdx.x * kZWarps + wib,
+                    zsm + wib * zpad(32 * CH));
+}
+
+// Ensemble form: item (inst, block index); the instance's chunk size picks
+// the instantiation, so each channel is solved exactly as on its own.
+__global__ void __launch_bounds__(kZWarps * 32) k_zsolve_ens(const EnsInst *__restrict__ ins,
+                                                             const EnsItem *__restrict__ items,
+                                                             int lvl, int max_ch)
+{
+    extern __shared__ double zsm[];
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    const SlcParams &P = I.P;
+    const int wib = threadIdx.x >> 5;
+    const long long wid = (long long)it.a * kZWarps + wib;
+    double *sm = zsm + wib * zpad(32 * max_ch);
+    double *u = I.lev[lvl][0], *v = I.lev[lvl][1], *w = I.lev[lvl][2];
+    switch (zsolve_chunk(P.nz)) {
+    case 1: zsolve_warp<1>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
+    case 2: zsolve_warp<2>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
+    case 4: zsolve_warp<4>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
+    case 8: zsolve_warp<8>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
+    case 12: zsolve_warp<12>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
+    case 16: zsolve_warp<16>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
+    default: zsolve_warp<32>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
     }
 }
 
@@ -285,4 +321,21 @@ extern "C" int slc_zsolve_noalloc(int nx, int ny, int nz, double nu, int top_wal
         return slc_report_error(SLC_E_CUDA, (std::string("slc_zsolve_noalloc: ") +
                                              cudaGetErrorString(e)).c_str());
     return SLC_OK;
+}
+
+int zsolve_ens_warps() { return kZWarps; }
+
+cudaError_t launch_zsolve_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                              int max_ch, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    const size_t smem = (size_t)kZWarps * zpad(32 * max_ch) * sizeof(double);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_zsolve_ens, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_zsolve_ens<<<nitems, kZWarps * 32, smem, s>>>(ins, items, lvl, max_ch);
+    count_launches(1);
+    return cudaGetLastError();
 }
