@@ -201,7 +201,8 @@ SLC_API int slc_bulk_shift(slc_grid *g, double *u, double *v, double *w, double 
 /* One BDF1 bootstrap step up to (not including) the bulk shift:
  * next <- advect(cur; U* = cur, dt) + dt R(cur); z-solve at dt; projection
  * at dt; p <- phi.  cur gets its BCs applied first.  The caller afterwards
- * treats cur as V^{n-1} and next as V^n.
+ * treats cur as V^{n-1} and next as V^n.  next's w wall faces must hold 0 on
+ * entry (the divergence reads them before the ghost refresh).
  * Replaces SLChannelFlow._step_sl_bdf1_bootstrap (solver.py:729-811)
  * without its final _bdf2_forcing_update call. */
 SLC_API int slc_step_bdf1(slc_grid *g, double *const cur[3], double *const next[3], double *p, double dt,
@@ -209,7 +210,10 @@ SLC_API int slc_step_bdf1(slc_grid *g, double *const cur[3], double *const next[
 
 /* One BDF2 step up to (not including) the bulk shift: slc_trace_gather_bdf2
  * into next, z-solve at 2dt/3, projection at 2dt/3, p <- phi.  The caller
- * afterwards rotates (prev, cur, next) <- (cur, next, prev).
+ * afterwards rotates (prev, cur, next) <- (cur, next, prev).  As in
+ * slc_step_bdf1, next's w wall faces must hold 0 on entry (a zeroed buffer
+ * or one from an earlier step): the divergence reads them before the ghost
+ * refresh.
  * Replaces SLChannelFlow.step_sl_bdf2 (solver.py:813-1018, noninc pressure)
  * without its final _bdf2_forcing_update call. */
 SLC_API int slc_step_bdf2(slc_grid *g, double *const cur[3], double *const prev[3], double *const next[3],
@@ -237,6 +241,31 @@ SLC_API int slc_timing_read(slc_grid *g, double *ms, int64_t *count);
 /* Number of kernels this library has launched in the process so far (its
  * own kernels; cuFFT's are not counted). */
 SLC_API int64_t slc_kernel_launches(void);
+
+/* ---- Adjoint (reverse mode) of the step ----------------------------------------
+ * No counterpart in the reference, which relies on torch autograd through its
+ * eager path.  Gradients of a loss on the velocity with respect to earlier
+ * velocities, FP64 handles only.  Adjoint fields lam_* are ghost-shaped like
+ * the velocity; their ghost entries may hold contributions that belong to
+ * interior values until slc_adjoint_bc folds them in. */
+
+/* Transpose of the ghost refresh (apply_bc_all, solver.py:70-107): add each
+ * ghost's adjoint, with the copy's sign, to its interior source, and zero
+ * every ghost (and w wall) entry. */
+SLC_API int slc_adjoint_bc(slc_grid *g, double *lam_u, double *lam_v, double *lam_w, void *stream);
+
+/* Reverse of one step.
+ *  - mode 2: slc_step_bdf2 + slc_bulk_shift, from cur = V^n and prev = V^{n-1};
+ *  - mode 1: the BDF1 bootstrap slc_step_bdf1 + slc_bulk_shift, from cur = V^0
+ *    (prev and lam_prev unused).
+ * cur and prev are the forward's states with their ghosts refreshed.
+ * lam_next = dJ/dV^{n+1} is consumed (overwritten as workspace).  The step's
+ * contributions are ADDED to lam_cur (dJ/dV^n) and lam_prev (dJ/dV^{n-1}).
+ * The transposed gathers are deterministic (no floating-point atomics).
+ * Allocates its workspace on first use. */
+SLC_API int slc_adjoint_step(slc_grid *g, int mode, double *const cur[3], double *const prev[3],
+                             double *const lam_next[3], double *const lam_cur[3],
+                             double *const lam_prev[3], double dt, void *stream);
 
 /* ---- Ensembles of independent channels --------------------------------------
  * No counterpart in the reference, which advances one channel per process.

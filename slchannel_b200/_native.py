@@ -79,6 +79,9 @@ SIGNATURES = {
     "slc_timing_read": ([_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_L)], _I),
     "slc_kernel_launches": ([], _L),
     "slc_zsolve_noalloc": ([_I, _I, _I, _D, _I, _P, _P, _D, _P, _P, _P, _P], _I),
+    "slc_adjoint_bc": ([_P, _P, _P, _P, _P], _I),
+    "slc_adjoint_step": ([_P, _I, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                          ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P], _I),
     "slc_ensemble_create": ([ctypes.POINTER(GridDesc), _I, ctypes.POINTER(_P)], _I),
     "slc_ensemble_destroy": ([_P], _I),
     "slc_ensemble_size": ([_P], _I),

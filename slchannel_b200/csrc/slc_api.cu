@@ -460,6 +460,7 @@ int slc_grid_destroy(slc_grid *g)
     }
     for (cudaEvent_t e : g->evs) cudaEventDestroy(e);
     for (void *p : g->allocs) cudaFree(p);
+    if (g->adj) adj_free(g->adj);
     delete g;
     return SLC_OK;
 }

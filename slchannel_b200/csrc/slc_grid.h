@@ -10,6 +10,9 @@
 #include "../../include/slc_b200.h"
 #include "slc_internal.h"
 
+struct AdjWS;                 // adjoint workspace (adjoint.cu), allocated on first use
+void adj_free(AdjWS *w);
+
 struct slc_grid {
     SlcParams P{};
     int device = 0;
@@ -29,6 +32,7 @@ struct slc_grid {
     int mixed = 0;          // SLC_PREC_MIXED
     bool mixed_ready = false;
     MixedWS mws{};
+    AdjWS *adj = nullptr;
     size_t ghost_elems[4] = {0, 0, 0, 0};
     cufftHandle fwd = 0, inv = 0;
     bool plans = false;
