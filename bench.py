@@ -54,6 +54,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     ap.add_argument("--mixed-error-steps", type=int, default=20)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-channel ensemble form")
+    ap.add_argument("--ensemble-n", type=int, default=48)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout check")
+    ap.add_argument("--adjoint-fd-dirs", type=int, default=16)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0,
                     help="CPU seconds the cpu_baseline sample aims for")
     return ap.parse_args()
@@ -433,6 +437,120 @@ def measure_mixed(flow64, n, order, K, W, dist):
             "form": "FP32 fluctuation about FP64 plane means in trace+gather; rest FP64"}
 
 
+def measure_ensemble(n_inst, K):
+    """The ensemble form: n_inst seeded channels (per-axis sizes from
+    {32, 48, 64, 96, 128}, gamma in [1.6, 2.2], Re_b in [2000, 5000], dt at
+    trajectory CFL 3, order 6, FP64) advanced by one CUDA-graph step, against
+    the loop over the same channels' single-channel solvers."""
+    import torch
+
+    from slchannel_b200.ensemble import ChannelEnsemble, ensemble_specs, loop_step, make_flow
+
+    specs = ensemble_specs(n_inst, seed=4)
+    flows, dts = [], []
+    for s in specs:
+        f, dt = make_flow(s, order=6)
+        f.step_sl_bdf2(dt)
+        flows.append(f)
+        dts.append(dt)
+    ens = ChannelEnsemble(flows, dts, use_graph=True, autotune=True)
+
+    def timed(fn, k):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(k):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / k
+
+    k = max(3, min(K, 20))
+    ms_graph = timed(ens.step, k)
+    ms_loop = timed(lambda: loop_step(flows, dts), max(3, k // 2))
+    pts = ens.points()
+    tiles = {}
+    for shape, (tk, _) in (ens.tune_ms or {}).items():
+        tiles[str(tk)] = tiles.get(str(tk), 0) + 1
+    out = {"value": 1000.0 / ms_graph, "unit": "ensemble steps/s", "ms_per_step": ms_graph,
+           "instances": n_inst, "points": pts,
+           "mpoint_updates_per_s": 3 * pts / (ms_graph / 1000.0) / 1e6,
+           "loop_ms_per_step": ms_loop, "speedup_vs_loop": ms_loop / ms_graph,
+           "autotuned_tile_z_extents": tiles,
+           "workload": f"{n_inst} channels, sizes from {{32,48,64,96,128}} per axis, 2pi x pi x 2, "
+                       "gamma U[1.6,2.2], Re_b U[2000,5000], dt at trajectory CFL 3, order 6, FP64"}
+    ens.close()
+    del flows, ens
+    torch.cuda.empty_cache()
+    return out
+
+
+def measure_adjoint(n_dirs):
+    """The adjoint form on 128 x 96 x 128 (2pi x pi x 2, Re_b 2800, dt 0.01,
+    order 6, FP64): 50-step rollout from the seeded synthetic field, loss =
+    kinetic energy of the final velocity weighted by a seeded smooth mask in
+    (0, 1), gradient w.r.t. the initial velocity through the hand-written
+    adjoint with checkpoints every 10 steps, checked against central finite
+    differences (h = 1e-6) in n_dirs seeded smooth directions."""
+    import torch
+
+    from slchannel_b200 import adjoint as A
+    from slchannel_b200.fields import synthetic_channel_field
+    from slchannel_b200.solver import SLChannelFlow
+    from slchannel_b200.utils import compute_bulk_velocity
+
+    nx, ny, nz, Lx, Ly, dt, steps, K = 128, 96, 128, 2 * math.pi, math.pi, 0.01, 50, 10
+    cfg = {"grid": {"nx": nx, "ny": ny, "nz": nz},
+           "domain": {"Lx": Lx, "Ly": Ly, "Lz": LZ, "stretching_type": "symmetric"},
+           "flow": {"Re": 2800.0, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": GAMMA},
+           "initialization": {"type": "parabolic"}, "time": {"dt": dt},
+           "compute": {"device": "cuda"},
+           "sl": {"interp_order": 6, "n_traj_iters": 2, "interp_dtype": "fp64"}}
+    flow = SLChannelFlow(config=cfg)
+    u, v, w = synthetic_channel_field(nx, ny, nz, Lx, Ly, LZ, flow.z_f.cpu().numpy(),
+                                      flow.z_c.cpu().numpy(), urms=0.1, seed=5)
+    flow.set_state(*(torch.from_numpy(a) for a in (u, v, w)))
+    flow.apply_bc_uvw()
+    flow.u *= 1.0 / float(compute_bulk_velocity(flow.u, flow.cell_vol_ratio, flow.total_volume))
+    flow._save_and_project_initial()
+    V0 = tuple(t.clone() for t in (flow.u, flow.v, flow.w))
+    mask = A.smooth_mask(flow, seed=6)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b)
+
+    A.gradient(flow, V0, dt, 2, mask, checkpoint_every=1)  # warm-up (workspaces, plans)
+    _, ms_fwd = timed(lambda: A.loss_of(flow, V0, dt, steps, mask))
+    (J, grad), ms_grad = timed(lambda: A.gradient(flow, V0, dt, steps, mask, checkpoint_every=K))
+    errs, worst = [], 0.0
+    for i in range(n_dirs):
+        d = A.random_direction(flow, seed=1000 + i)
+        fd = A.central_fd(flow, V0, d, 1e-6, dt, steps, mask)
+        ad = A.dot(grad, d)
+        e = abs(fd - ad) / max(abs(fd), 0.1)
+        errs.append(e)
+        worst = max(worst, e)
+    out = {"grid": [nx, ny, nz], "steps": steps, "checkpoint_every": K, "loss": J,
+           "forward_ms": ms_fwd, "gradient_ms": ms_grad,
+           "adjoint_ms_per_step": (ms_grad - ms_fwd) / steps,
+           "backward_over_forward": (ms_grad - ms_fwd) / ms_fwd,
+           "fd_directions": n_dirs, "fd_h": 1e-6, "fd_max_rel_err": worst,
+           "fd_median_rel_err": sorted(errs)[len(errs) // 2],
+           "workload": "128x96x128, 2pi x pi x 2, Re_b 2800, dt 0.01, order 6, FP64, 50 steps, "
+                       "checkpoints every 10, loss = masked kinetic energy of V^50"}
+    del flow, V0, grad
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_b200(args):
     import torch
 
@@ -554,6 +672,10 @@ def run_b200(args):
         "gpu_launches": int(launches), "roofline": roofline, "clocks": clocks, "e2e": e2e,
         "mixed": mixed,
     }
+    if world == 1 and not args.no_ensemble:
+        line["ensemble"] = measure_ensemble(args.ensemble_n, K)
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = measure_adjoint(args.adjoint_fd_dirs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_cpu, desc, threads = cpu_step_sample(n, order, args.cpu_budget_s)
         line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": UNIT, "cores": threads, "kind": "port",
