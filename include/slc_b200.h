@@ -238,6 +238,13 @@ SLC_API int slc_timing(slc_grid *g, int enable);
  * ms and count each hold SLC_NPHASE entries. */
 SLC_API int slc_timing_read(slc_grid *g, double *ms, int64_t *count);
 
+/* Counters of the shared-memory-staged BDF2 gather (nz >= 39), accumulated
+ * since creation or the last reset: out4[0] staged boxes that did not arrive
+ * within the poll limit (the block then gathered through L1; results are
+ * unaffected), out4[1] blocks, out4[2] near-foot boxes staged, out4[3]
+ * far-foot boxes staged (the rest gathered through L1).  Synchronous. */
+SLC_API int slc_gather_stats(slc_grid *g, int64_t *out4, int reset);
+
 /* Number of kernels this library has launched in the process so far (its
  * own kernels; cuFFT's are not counted). */
 SLC_API int64_t slc_kernel_launches(void);

@@ -1,0 +1,423 @@
+// sl_tma.cu -- the BDF2 trace+gather with the gather's source boxes staged
+// in shared memory by the Tensor Memory Accelerator (sm_100a).
+//
+// Why: the order-6 gather issues 216 eight-byte loads per foot per arrival
+// point.  A warp's load at one stencil offset covers 32 consecutive z values
+// (256 bytes), which from L1 costs about three wavefronts (it straddles three
+// 128-byte lines at most alignments) and from shared memory two, conflict-
+// free at any alignment.  The kernel is bound by that data pipe.
+//
+// How: a block is a tile of 2 (x) x 4 (y) x 32 (z) arrival points, one warp
+// per 32 z.  Every thread traces both feet (the iterated midpoint rule of
+// sl_device.cuh, unchanged).  Shared-memory integer min/max of the feet's
+// stencil bases give each foot's bounding box.  If it fits the fixed box of
+// kBX x kBY x kBZ nodes, one thread issues a 3-D cp.async.bulk.tensor load of
+// the box (no multicast) from a halo-padded node copy of V^n (near foot) or
+// V^{n-1} (far foot) onto an mbarrier, and the threads gather from shared
+// memory.  A block whose feet spread wider uses the L1 gather.  The boxes
+// come from padded node copies, written together with U* by k_mid_pack:
+// node (i, j, k) at padded (i + q nx, j + r ny, k), x and y extended by one
+// box, so a box never wraps.  Weights, the contraction order and the
+// epilogue are those of k_sl, so the results are bit-identical to it.
+#include <cuda.h>
+
+#include <climits>
+#include <mutex>
+
+#include "slc_grid.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+#include "sl_device.cuh"
+
+constexpr int kTI = 2, kTJ = 4, kTK = 32;    // arrival tile (x, y, z)
+constexpr int kBX = 10, kBY = 12, kBZ = 40;  // staged box (x, y, z) in nodes
+constexpr int kBoxElems = kBX * kBY * kBZ;
+constexpr size_t kBoxBytes = (size_t)kBoxElems * sizeof(double);
+constexpr size_t kSmemBytes = 2 * kBoxBytes + 1024;  // + alignment slack
+constexpr int kWaitLimit = 1 << 20;                  // bounded mbarrier polls
+
+static_assert(kTI * kTJ * kTK == kThreads, "one thread per arrival point");
+static_assert((kBZ * sizeof(double)) % 16 == 0, "TMA inner box extent");
+
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+// Poll phase 0 of the barrier at most kWaitLimit times; false on time-out.
+__device__ __forceinline__ bool mbar_wait(unsigned bar)
+{
+    for (int it = 0; it < kWaitLimit; ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(0u)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap *tm, int c0, int c1, int c2,
+                                            unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"((unsigned long long)tm), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+// Unwrapped stencil base of one coordinate relative to the tile origin
+// (NaN or far-out values give a large sentinel that no box fits).
+__device__ __forceinline__ int rel_base(double f, int h, int origin)
+{
+    const double r = f - (double)h - (double)origin;
+    if (!(r > -4096.0 && r < 4096.0)) return 1 << 20;
+    return (int)r;
+}
+
+struct Foot {
+    double z;      // clamped z
+    double tx, ty;
+    int rx, ry;    // unwrapped x, y base (minus O/2 - 1) relative to the tile
+    int k0;        // z base
+};
+
+template <int C, int O>
+__device__ __forceinline__ Foot locate_foot(const SlcParams &P, double xd, double yd, double zd,
+                                            int i0, int j0, unsigned &ncl)
+{
+    constexpr int h = O / 2 - 1;
+    if (zd < P.z_lo || zd > P.z_hi) ncl += 1;
+    Foot F;
+    F.z = clampz(P, zd);
+    double s = xd * P.inv_dx + Comp<C>::shift_x;
+    double f = floor(s);
+    F.tx = s - f;
+    F.rx = rel_base(f, h, i0);
+    s = yd * P.inv_dy + Comp<C>::shift_y;
+    f = floor(s);
+    F.ty = s - f;
+    F.ry = rel_base(f, h, j0);
+    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
+    const int m0 = locate_m0(P, Comp<C>::centers, face_cell(P, F.z), F.z);
+    F.k0 = min(max(m0 - h, 0), NZ - O);
+    return F;
+}
+
+// Gather from a staged box: weights and contraction order as gather_sum.
+template <int C, int O>
+__device__ __forceinline__ double gather_box(const SlcParams &P, const double *box, const Foot &F,
+                                             int ox, int oy, int oz)
+{
+    double wx[O], wy[O], wz[O];
+    uniform_weights<O, double>(P, F.tx, wx);
+    uniform_weights<O, double>(P, F.ty, wy);
+    const double *zn = Comp<C>::centers ? P.zc : P.zf;
+    const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
+    z_weights<O, double>(zn, dinv, F.k0, F.z, wz);
+    const double *b = box + (ox * kBY + oy) * kBZ + oz;
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < O; ++i) {
+        double accy = 0.0;
+#pragma unroll
+        for (int j = 0; j < O; ++j) {
+            const double *row = b + (i * kBY + j) * kBZ;
+            double accz = 0.0;
+#pragma unroll
+            for (int k = 0; k < O; ++k) accz = fma(wz[k], row[k], accz);
+            accy = fma(wy[j], accz, accy);
+        }
+        acc = fma(wx[i], accy, acc);
+    }
+    return acc;
+}
+
+// Gather through L1 from the ghost-shaped array (the k_sl path).
+template <int C, int O>
+__device__ __forceinline__ double gather_global(const SlcParams &P, NodeView<double> V, double xd,
+                                                double yd, const Foot &F)
+{
+    Stencil<O, double> st;
+    build_stencil<C, O, double>(P, V.sx, V.sy, xd, yd, F.z, face_cell(P, F.z), st);
+    return gather_sum<O, double, double>(V.p, st);
+}
+
+template <int C, int O>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_sl_tma(SlcParams P, Vel3 M, const double *__restrict__ fn, const double *__restrict__ fnm1,
+             double dt, double *__restrict__ out, unsigned long long *nclamp, unsigned long long *stats,
+             const __grid_constant__ CUtensorMap tmN, const __grid_constant__ CUtensorMap tmM)
+{
+    extern __shared__ unsigned char smraw[];
+    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ int red[12];  // per foot: min/max of rx, ry, k0
+    double *boxN = (double *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    double *boxM = boxN + kBoxElems;
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.z * kTI, j0 = blockIdx.y * kTJ;
+    const int k = blockIdx.x * kTK + (tid & 31);
+    const int j = j0 + ((tid >> 5) & (kTJ - 1));
+    const int i = i0 + (tid >> 7);
+    const int nzi = (C == 2) ? P.nz - 1 : P.nz;
+    const bool act = k < nzi && j < P.ny && i < P.nx;
+    const unsigned barN = smem_u32(&mbar[0]), barM = smem_u32(&mbar[1]);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            red[2 * q] = INT_MAX;
+            red[2 * q + 1] = INT_MIN;
+        }
+        mbar_init(barN, 1);
+        mbar_init(barM, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    unsigned ncl = 0;
+    double xa = 0.0, ya = 0.0, za = 0.0, us0 = 0.0, vs0 = 0.0, ws0 = 0.0;
+    double xn = 0.0, yn = 0.0, zn = 0.0, xm = 0.0, ym = 0.0, zm = 0.0;
+    Foot Fn{}, Fm{};
+    if (act) {
+        arrival_point<C>(P, i, j, k, xa, ya, za);
+        arrival_sample<C>(P, M, i, j, k, NodeValF64(), us0, vs0, ws0);
+        trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xn, yn, zn);
+        trace_foot(P, M, xa, ya, za, dt, us0, vs0, ws0, xm, ym, zm);  // half of 2 dt
+        Fn = locate_foot<C, O>(P, xn, yn, zn, i0, j0, ncl);
+        Fm = locate_foot<C, O>(P, xm, ym, zm, i0, j0, ncl);
+        atomicMin(&red[0], Fn.rx);
+        atomicMax(&red[1], Fn.rx);
+        atomicMin(&red[2], Fn.ry);
+        atomicMax(&red[3], Fn.ry);
+        atomicMin(&red[4], Fn.k0);
+        atomicMax(&red[5], Fn.k0);
+        atomicMin(&red[6], Fm.rx);
+        atomicMax(&red[7], Fm.rx);
+        atomicMin(&red[8], Fm.ry);
+        atomicMax(&red[9], Fm.ry);
+        atomicMin(&red[10], Fm.k0);
+        atomicMax(&red[11], Fm.k0);
+    }
+    __syncthreads();
+    // block-uniform box choice per foot
+    bool fit[2];
+    int X0[2] = {0, 0}, Y0[2] = {0, 0}, Z0[2] = {0, 0};
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        const int *r = red + 6 * f;
+        fit[f] = r[0] <= r[1] && r[1] - r[0] + O <= kBX && r[3] - r[2] + O <= kBY &&
+                 r[5] + O - (r[4] & ~1) <= kBZ;
+        if (fit[f]) {  // r[0], r[2] are small here (|.| < 4096)
+            int x0 = (i0 + r[0]) % P.nx;
+            if (x0 < 0) x0 += P.nx;
+            int y0 = (j0 + r[2]) % P.ny;
+            if (y0 < 0) y0 += P.ny;
+            X0[f] = x0;
+            Y0[f] = y0;
+            Z0[f] = r[4] & ~1;  // even: 16-byte aligned inner coordinate
+        }
+    }
+    if (tid == 0) {
+        // stats: [0] time-outs, [1] blocks, [2] near boxes staged, [3] far boxes staged
+        atomicAdd(stats + 1, 1ull);
+        if (fit[0]) atomicAdd(stats + 2, 1ull);
+        if (fit[1]) atomicAdd(stats + 3, 1ull);
+        if (fit[0]) {
+            mbar_expect_tx(barN, (unsigned)kBoxBytes);
+            tma_load_3d(smem_u32(boxN), &tmN, Z0[0], Y0[0], X0[0], barN);
+        }
+        if (fit[1]) {
+            mbar_expect_tx(barM, (unsigned)kBoxBytes);
+            tma_load_3d(smem_u32(boxM), &tmM, Z0[1], Y0[1], X0[1], barM);
+        }
+    }
+    if (act) {
+        double ubar, ubb;
+        bool staged = fit[0] && mbar_wait(barN);
+        if (fit[0] && !staged) atomicAdd(stats, 1ull);
+        if (staged)
+            ubar = gather_box<C, O>(P, boxN, Fn, Fn.rx - red[0], Fn.ry - red[2], Fn.k0 - Z0[0]);
+        else
+            ubar = gather_global<C, O>(P, ghost_view<double>(C, fn, P.nx, P.ny, P.nz), xn, yn, Fn);
+        staged = fit[1] && mbar_wait(barM);
+        if (fit[1] && !staged) atomicAdd(stats, 1ull);
+        if (staged)
+            ubb = gather_box<C, O>(P, boxM, Fm, Fm.rx - red[6], Fm.ry - red[8], Fm.k0 - Z0[1]);
+        else
+            ubb = gather_global<C, O>(P, ghost_view<double>(C, fnm1, P.nx, P.ny, P.nz), xm, ym, Fm);
+        const double Rn = xy_diffusion<C>(P, fn, i, j, k);
+        const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion<C>(P, fnm1, i, j, k);
+        double res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
+        res = res + ((2.0 / 3.0) * dt) * Rh;
+        const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
+        out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
+    }
+    add_clamps(nclamp, ncl);
+    // no copy may still be writing this block's shared memory when it exits
+    if (tid == 0) {
+        if (fit[0]) mbar_wait(barN);
+        if (fit[1]) mbar_wait(barM);
+    }
+}
+
+// U* = 2 V^n - V^{n-1} at every node (ghost-shaped, node entries only) and
+// the halo-padded node copies of V^n and V^{n-1}; one thread per padded
+// element (x fastest last: z contiguous in both layouts).
+template <int C>
+__global__ void k_mid_pack(SlcParams P, const double *__restrict__ a, const double *__restrict__ b,
+                           double ca, double cb, double *__restrict__ mid, double *__restrict__ pa,
+                           double *__restrict__ pb, int NZp)
+{
+    const int NZ = C < 2 ? P.nz + 2 : P.nz + 1;
+    const int PX = P.nx + kBX, PY = P.ny + kBY;
+    const long long n = (long long)PX * PY * NZp;
+    const NodeView<double> Va = ghost_view<double>(C, a, P.nx, P.ny, P.nz);
+    const NodeView<double> Vb = ghost_view<double>(C, b, P.nx, P.ny, P.nz);
+    double *vm = const_cast<double *>(ghost_view<double>(C, mid, P.nx, P.ny, P.nz).p);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int z = (int)(t % NZp);
+        const long long q = t / NZp;
+        const int y = (int)(q % PY), x = (int)(q / PY);
+        if (z >= NZ) {
+            pa[t] = 0.0;
+            pb[t] = 0.0;
+            continue;
+        }
+        const int xi = x % P.nx, yj = y % P.ny;
+        const size_t g = (size_t)xi * Va.sx + (size_t)yj * Va.sy + z;
+        const double va = Va.p[g], vb = Vb.p[g];
+        pa[t] = va;
+        pb[t] = vb;
+        if (x < P.nx && y < P.ny) vm[g] = ca * va + cb * vb;
+    }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static std::once_flag once;
+    static EncodeTiledFn fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+template <int O>
+cudaError_t launch_tma_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
+                         unsigned long long *ncl, unsigned long long *stats, const TmaSL &T,
+                         cudaStream_t s)
+{
+    const dim3 gc((P.nz + kTK - 1) / kTK, (P.ny + kTJ - 1) / kTJ, (P.nx + kTI - 1) / kTI);
+    const dim3 gw((P.nz - 1 + kTK - 1) / kTK, (P.ny + kTJ - 1) / kTJ, (P.nx + kTI - 1) / kTI);
+    // per device context, so set on every launch (a host-side attribute write)
+    cudaError_t attr = cudaFuncSetAttribute(k_sl_tma<0, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    if (attr == cudaSuccess)
+        attr = cudaFuncSetAttribute(k_sl_tma<1, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    if (attr == cudaSuccess)
+        attr = cudaFuncSetAttribute(k_sl_tma<2, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    if (attr != cudaSuccess) return attr;
+    const CUtensorMap *tm = (const CUtensorMap *)T.maps;
+    k_sl_tma<0, O><<<gc, kThreads, kSmemBytes, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl, stats, tm[0], tm[3]);
+    k_sl_tma<1, O><<<gc, kThreads, kSmemBytes, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl, stats, tm[1], tm[4]);
+    if (P.nz > 1)
+        k_sl_tma<2, O><<<gw, kThreads, kSmemBytes, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl, stats, tm[2], tm[5]);
+    count_launches(P.nz > 1 ? 3 : 2);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int tma_padded_nz(int NZ) { return (NZ + 1) & ~1; }
+
+// Boxes must fit inside the padded arrays in every dimension.
+bool tma_supported(const SlcParams &P) { return P.nz + 1 >= kBZ && encode_fn() != nullptr; }
+
+size_t tma_padded_elems(const SlcParams &P, int comp)
+{
+    const int NZ = comp < 2 ? P.nz + 2 : P.nz + 1;
+    return (size_t)(P.nx + kBX) * (P.ny + kBY) * tma_padded_nz(NZ);
+}
+
+// Tensor maps of the six padded node copies (slot comp + 3 * which).
+cudaError_t tma_encode(const SlcParams &P, TmaSL &T)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    static_assert(sizeof(CUtensorMap) * 6 <= sizeof(T.maps), "tensor-map storage");
+    CUtensorMap *tm = (CUtensorMap *)T.maps;
+    for (int q = 0; q < 6; ++q) {
+        const int comp = q % 3;
+        const int NZ = comp < 2 ? P.nz + 2 : P.nz + 1;
+        const cuuint64_t nzp = (cuuint64_t)tma_padded_nz(NZ);
+        const cuuint64_t dims[3] = {nzp, (cuuint64_t)(P.ny + kBY), (cuuint64_t)(P.nx + kBX)};
+        const cuuint64_t strides[2] = {nzp * 8, nzp * 8 * (cuuint64_t)(P.ny + kBY)};
+        const cuuint32_t box[3] = {(cuuint32_t)kBZ, (cuuint32_t)kBY, (cuuint32_t)kBX};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        CUresult r = enc(&tm[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)T.pad[q], dims, strides, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_mid_pack(const SlcParams &P, Tri cur, Tri prev, TriMut mid, const TmaSL &T,
+                            cudaStream_t s)
+{
+    for (int c = 0; c < 3; ++c) {
+        const int NZ = c < 2 ? P.nz + 2 : P.nz + 1;
+        const int nzp = tma_padded_nz(NZ);
+        const long long n = (long long)tma_padded_elems(P, c);
+        long long blocks = (n + 255) / 256;
+        if (blocks > 148 * 16) blocks = 148 * 16;
+        const double *a = c == 0 ? cur.u : (c == 1 ? cur.v : cur.w);
+        const double *b = c == 0 ? prev.u : (c == 1 ? prev.v : prev.w);
+        double *m = c == 0 ? mid.u : (c == 1 ? mid.v : mid.w);
+        if (c == 0) k_mid_pack<0><<<(unsigned)blocks, 256, 0, s>>>(P, a, b, 2.0, -1.0, m, T.pad[c], T.pad[c + 3], nzp);
+        else if (c == 1) k_mid_pack<1><<<(unsigned)blocks, 256, 0, s>>>(P, a, b, 2.0, -1.0, m, T.pad[c], T.pad[c + 3], nzp);
+        else k_mid_pack<2><<<(unsigned)blocks, 256, 0, s>>>(P, a, b, 2.0, -1.0, m, T.pad[c], T.pad[c + 3], nzp);
+    }
+    count_launches(3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sl_tma(const SlcParams &P, Tri fn, Tri fnm1, Tri mid, double dt, TriMut out,
+                          unsigned long long *nclamp, unsigned long long *stats, const TmaSL &T,
+                          cudaStream_t s)
+{
+    Vel3 M;
+    M.u = ghost_view<double>(0, mid.u, P.nx, P.ny, P.nz);
+    M.v = ghost_view<double>(1, mid.v, P.nx, P.ny, P.nz);
+    M.w = ghost_view<double>(2, mid.w, P.nx, P.ny, P.nz);
+    if (P.order == 4) return launch_tma_t<4>(P, M, fn, fnm1, dt, out, nclamp, stats, T, s);
+    return launch_tma_t<6>(P, M, fn, fnm1, dt, out, nclamp, stats, T, s);
+}

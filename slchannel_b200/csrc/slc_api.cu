@@ -153,6 +153,25 @@ int ensure_mid(slc_grid *g)
     return SLC_OK;
 }
 
+// Padded node copies and tensor maps of the TMA-staged BDF2 gather; state -1
+// (L1 gather) when the grid is too shallow for a box or the driver lacks the
+// tensor-map entry point.
+int ensure_tma(slc_grid *g)
+{
+    if (g->tma_state) return SLC_OK;
+    if (!tma_supported(g->P)) {
+        g->tma_state = -1;
+        return SLC_OK;
+    }
+    for (int q = 0; q < 6; ++q) {
+        int rc = dalloc(g, &g->tma.pad[q], tma_padded_elems(g->P, q % 3), "padded node copy");
+        if (rc) return rc;
+    }
+    SLC_CK(tma_encode(g->P, g->tma), "tensor map encode");
+    g->tma_state = 1;
+    return SLC_OK;
+}
+
 int ensure_mixed(slc_grid *g)
 {
     if (g->mixed_ready) return SLC_OK;
@@ -237,7 +256,24 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
         return SLC_OK;
     }
     int rc = ensure_mid(g);
+    if (!rc) rc = ensure_tma(g);
     if (rc) return rc;
+    if (g->tma_state == 1) {
+        long t = tim_begin(g, SLC_PHASE_MID, s);
+        SLC_CK(launch_mid_pack(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
+                               TriMut{g->mid[0], g->mid[1], g->mid[2]}, g->tma, s),
+               "U* and padded node copies");
+        tim_end(g, t, s);
+        unsigned long long *ncl = counter(g, nclamp);
+        SLC_CK(cudaMemsetAsync(ncl, 0, sizeof(unsigned long long), s), "memset");
+        t = tim_begin(g, SLC_PHASE_SL, s);
+        SLC_CK(launch_sl_tma(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
+                             Tri{g->mid[0], g->mid[1], g->mid[2]}, dt, TriMut{out[0], out[1], out[2]},
+                             ncl, g->dev_flags, g->tma, s),
+               "trace+gather BDF2 (TMA-staged)");
+        tim_end(g, t, s);
+        return SLC_OK;
+    }
     long t = tim_begin(g, SLC_PHASE_MID, s);
     for (int c = 0; c < 3; ++c)
         SLC_CK(launch_lincomb(cur[c], prev[c], 2.0, -1.0, g->mid[c], (int64_t)g->ghost_elems[c], s),
@@ -427,6 +463,11 @@ int slc_grid_create(const slc_grid_desc *d, slc_grid **out)
     CREATE_CK(dalloc(g, &g->zs_tab, zsolve_table_doubles(nz), "z-solve tables"));
     CREATE_CK(dalloc(g, &g->partials, (size_t)kBulkBlocks, "bulk partials"));
     CREATE_CK(dalloc(g, &g->scal, (size_t)8, "scalars"));
+    CREATE_CK(dalloc(g, &g->dev_flags, (size_t)4, "device flags"));
+    if (cudaMemset(g->dev_flags, 0, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+        slc_grid_destroy(g);
+        return fail(nullptr, SLC_E_CUDA, "memset device flags");
+    }
     CREATE_CK(dalloc(g, &g->ncl_scratch, (size_t)1, "clamp counter"));
     for (int c = 0; c < 4; ++c) {
         GhostShape s = ghost_shape(c, nx, ny, nz);
@@ -712,6 +753,17 @@ int slc_step_bdf2(slc_grid *g, double *const cur[3], double *const prev[3], doub
     rc = do_zsolve(g, next[0], next[1], next[2], dt_eff, s);
     if (rc) return rc;
     return do_project(g, next[0], next[1], next[2], p, dt_eff, dt_eff, s);
+}
+
+int slc_gather_stats(slc_grid *g, int64_t *out4, int reset)
+{
+    if (!g || !out4) return fail(g, SLC_E_INVALID, "null argument");
+    DeviceGuard dg(g->device);
+    unsigned long long h[4];
+    SLC_CK(cudaMemcpy(h, g->dev_flags, sizeof(h), cudaMemcpyDeviceToHost), "read gather stats");
+    for (int q = 0; q < 4; ++q) out4[q] = (int64_t)h[q];
+    if (reset) SLC_CK(cudaMemset(g->dev_flags, 0, sizeof(h)), "reset gather stats");
+    return SLC_OK;
 }
 
 int slc_timing(slc_grid *g, int enable)

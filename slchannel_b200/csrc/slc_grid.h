@@ -33,6 +33,9 @@ struct slc_grid {
     bool mixed_ready = false;
     MixedWS mws{};
     AdjWS *adj = nullptr;
+    TmaSL tma{};
+    int tma_state = 0;        // 0 not tried, 1 ready, -1 unavailable (L1 gather path)
+    unsigned long long *dev_flags = nullptr;  // staged-gather statistics (launch_sl_tma)
     size_t ghost_elems[4] = {0, 0, 0, 0};
     cufftHandle fwd = 0, inv = 0;
     bool plans = false;

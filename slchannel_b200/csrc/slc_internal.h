@@ -153,3 +153,24 @@ cudaError_t launch_bulk_partials_ens(const EnsInst *ins, const EnsItem *items, i
                                      int lvl, int with_shift, cudaStream_t s);
 // mode 0: scal = [U_bulk - bulk, (U_bulk - bulk) / dt]; mode 1: bulk_out = [bulk, scal[1]].
 cudaError_t launch_bulk_finish_ens(const EnsInst *ins, int ninst, int mode, cudaStream_t s);
+
+// ---- sl_tma.cu: BDF2 trace+gather with TMA-staged source boxes ---------------
+// Halo-padded node copies of V^n (slots 0-2) and V^{n-1} (3-5) and their
+// tensor maps (CUtensorMap, 128 bytes each, stored opaquely here).
+struct TmaSL {
+    double *pad[6];
+    alignas(64) unsigned char maps[6 * 128];
+};
+int tma_padded_nz(int NZ);
+size_t tma_padded_elems(const SlcParams &P, int comp);
+bool tma_supported(const SlcParams &P);
+cudaError_t tma_encode(const SlcParams &P, TmaSL &T);
+// U* (node entries of the ghost-shaped mid arrays) and the padded copies.
+cudaError_t launch_mid_pack(const SlcParams &P, Tri cur, Tri prev, TriMut mid, const TmaSL &T,
+                            cudaStream_t s);
+// stats (device, accumulated): [0] staged boxes that did not arrive within
+// the poll limit (that block then gathers through L1; results stay exact),
+// [1] blocks, [2] near-foot boxes staged, [3] far-foot boxes staged.
+cudaError_t launch_sl_tma(const SlcParams &P, Tri fn, Tri fnm1, Tri mid, double dt, TriMut out,
+                          unsigned long long *nclamp, unsigned long long *stats, const TmaSL &T,
+                          cudaStream_t s);

@@ -83,6 +83,19 @@ def test_parity_ragged_grid(order):
                resync=False)
 
 
+@pytest.mark.parametrize("order", [6, 4])
+def test_parity_staged_gather_ragged(order):
+    """nz >= 39 takes the TMA-staged gather: partial x, y and z tiles, feet
+    across the periodic seams, both orders."""
+    run_parity(30, 18, 48, 2 * math.pi, math.pi, order, steps=4, dt=0.05, urms=0.15)
+
+
+def test_parity_staged_gather_wide_feet():
+    """Large dt: in many blocks the feet spread beyond the staged box and
+    those blocks gather through L1; wall clamps on both walls."""
+    run_parity(24, 16, 40, 2 * math.pi, math.pi, 6, steps=3, dt=0.6, urms=0.35)
+
+
 def test_parity_config1_64cubed_20_steps():
     """Config 1: 64^3 in 2pi x pi x 2, gamma 2, Re_b 2800, order 6, dt 0.01,
     20 steps (BDF1 bootstrap + 19 BDF2), free-running, against the oracle
