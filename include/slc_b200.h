@@ -128,6 +128,20 @@ SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *v
                           const double *unm1, const double *vnm1, const double *wnm1, double dt,
                           double *ou, double *ov, double *ow, int64_t *nclamp, void *stream);
 
+/* slc_trace_gather_bdf2 with each block's two gather source boxes staged
+ * in shared memory by the Tensor Memory Accelerator (3-D cp.async.bulk.tensor
+ * loads of halo-padded node copies written with U*; FP64 handles with
+ * nz >= 39, otherwise identical to slc_trace_gather_bdf2).  Results are
+ * bit-identical to slc_trace_gather_bdf2.  Not the step's default: at the
+ * 256^3 benchmark its shared-memory loads pay bank conflicts about equal to
+ * the L1 path's line splits, and the padded copies cost an extra pass.
+ * slc_gather_stats reports how many boxes were staged.  No counterpart in
+ * the reference. */
+SLC_API int slc_trace_gather_bdf2_staged(slc_grid *g, const double *un, const double *vn,
+                                         const double *wn, const double *unm1, const double *vnm1,
+                                         const double *wnm1, double dt, double *ou, double *ov,
+                                         double *ow, int64_t *nclamp, void *stream);
+
 /* theta = 1 implicit wall-normal diffusion, in place on the interiors:
  * (I - dt nu Dzz) f_new = f.
  * Replaces solve_implicit_diffusion_{u,v,w} (slchannel/operators.py:382-630). */
@@ -238,7 +252,7 @@ SLC_API int slc_timing(slc_grid *g, int enable);
  * ms and count each hold SLC_NPHASE entries. */
 SLC_API int slc_timing_read(slc_grid *g, double *ms, int64_t *count);
 
-/* Counters of the shared-memory-staged BDF2 gather (nz >= 39), accumulated
+/* Counters of slc_trace_gather_bdf2_staged, accumulated
  * since creation or the last reset: out4[0] staged boxes that did not arrive
  * within the poll limit (the block then gathered through L1; results are
  * unaffected), out4[1] blocks, out4[2] near-foot boxes staged, out4[3]

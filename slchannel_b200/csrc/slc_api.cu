@@ -236,7 +236,8 @@ int do_apply_bc(slc_grid *g, double *u, double *v, double *w, cudaStream_t s)
 }
 
 int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *const prev[3],
-                         double dt, double *const out[3], int64_t *nclamp, cudaStream_t s)
+                         double dt, double *const out[3], int64_t *nclamp, cudaStream_t s,
+                         bool staged = false)
 {
     if (g->mixed) {
         int rc = ensure_mixed(g);
@@ -256,9 +257,9 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
         return SLC_OK;
     }
     int rc = ensure_mid(g);
-    if (!rc) rc = ensure_tma(g);
+    if (!rc && staged) rc = ensure_tma(g);
     if (rc) return rc;
-    if (g->tma_state == 1) {
+    if (staged && g->tma_state == 1) {
         long t = tim_begin(g, SLC_PHASE_MID, s);
         SLC_CK(launch_mid_pack(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
                                TriMut{g->mid[0], g->mid[1], g->mid[2]}, g->tma, s),
@@ -596,6 +597,20 @@ int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *vn, const
     const double *cur[3] = {un, vn, wn}, *prev[3] = {unm1, vnm1, wnm1};
     double *out[3] = {ou, ov, ow};
     return do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, S(stream));
+}
+
+int slc_trace_gather_bdf2_staged(slc_grid *g, const double *un, const double *vn, const double *wn,
+                                 const double *unm1, const double *vnm1, const double *wnm1,
+                                 double dt, double *ou, double *ov, double *ow, int64_t *nclamp,
+                                 void *stream)
+{
+    if (!g) return fail(nullptr, SLC_E_INVALID, "null handle");
+    if (!un || !vn || !wn || !unm1 || !vnm1 || !wnm1 || !ou || !ov || !ow)
+        return fail(g, SLC_E_INVALID, "null pointer");
+    DeviceGuard dg(g->device);
+    const double *cur[3] = {un, vn, wn}, *prev[3] = {unm1, vnm1, wnm1};
+    double *out[3] = {ou, ov, ow};
+    return do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, S(stream), true);
 }
 
 int slc_zsolve(slc_grid *g, double *u, double *v, double *w, double dt, void *stream)

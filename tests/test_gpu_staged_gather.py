@@ -1,0 +1,82 @@
+"""slc_trace_gather_bdf2_staged (gather source boxes staged in shared memory
+by TMA) against slc_trace_gather_bdf2 (gather through L1): bit-identical
+outputs and clamp counts, with every box staged (small dt), with many blocks
+falling back to L1 (wide feet), and on a grid too shallow for a box."""
+
+import ctypes
+import math
+
+import pytest
+import torch
+
+from slchannel_b200 import _native as N
+from slchannel_b200.fields import synthetic_channel_field
+from slchannel_b200.solver import SLChannelFlow
+from slchannel_b200.utils import compute_bulk_velocity
+
+pytestmark = pytest.mark.gpu
+
+
+def _flow(n3, dt, urms, order=6):
+    nx, ny, nz = n3
+    cfg = {"grid": {"nx": nx, "ny": ny, "nz": nz},
+           "domain": {"Lx": 2 * math.pi, "Ly": math.pi, "Lz": 2.0},
+           "flow": {"Re": 2800.0, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": 2.0},
+           "initialization": {"type": "parabolic"}, "time": {"dt": dt},
+           "compute": {"device": "cuda"},
+           "sl": {"interp_order": order, "n_traj_iters": 2, "interp_dtype": "fp64"}}
+    f = SLChannelFlow(config=cfg)
+    u, v, w = synthetic_channel_field(nx, ny, nz, 2 * math.pi, math.pi, 2.0, f.z_f.cpu().numpy(),
+                                      f.z_c.cpu().numpy(), urms=urms, seed=3)
+    f.set_state(*(torch.from_numpy(a) for a in (u, v, w)))
+    f.apply_bc_uvw()
+    f.u *= 1.0 / float(compute_bulk_velocity(f.u, f.cell_vol_ratio, f.total_volume))
+    f._save_and_project_initial()
+    for _ in range(2):
+        f.step_sl_bdf2(dt)
+    return f
+
+
+def _both(f, dt):
+    cur, prev = (f.u, f.v, f.w), (f.u_nm1, f.v_nm1, f.w_nm1)
+    res = []
+    for name in ("slc_trace_gather_bdf2", "slc_trace_gather_bdf2_staged"):
+        out = [torch.zeros_like(t) for t in cur]
+        ncl = torch.zeros((), dtype=torch.int64, device=f.device)
+        f._grid.call(name, *[N.ptr(t) for t in cur], *[N.ptr(t) for t in prev], float(dt),
+                     *[N.ptr(t) for t in out], N.ptr(ncl), N.stream_of(f.u))
+        res.append((out, int(ncl)))
+    torch.cuda.synchronize()
+    stats = (ctypes.c_int64 * 4)()
+    N.lib().slc_gather_stats(f._grid.handle, stats, 1)
+    return res, list(stats)
+
+
+@pytest.mark.parametrize("order", [6, 4])
+def test_staged_equals_l1_all_staged(order):
+    f = _flow((40, 24, 48), 0.01, 0.1, order)
+    (a, na), (b, nb) = _both(f, 0.01)[0]
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    assert na == nb
+    stats = _both(f, 0.01)[1]
+    assert stats[0] == 0 and stats[1] > 0 and stats[2] == stats[1] and stats[3] == stats[1]
+
+
+def test_staged_equals_l1_wide_feet():
+    f = _flow((24, 16, 40), 0.6, 0.35)
+    (a, na), (b, nb) = _both(f, 0.6)[0]
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    assert na == nb and na > 0
+    stats = _both(f, 0.6)[1]
+    assert stats[0] == 0 and stats[3] < stats[1]  # some blocks gathered through L1
+
+
+def test_staged_on_a_shallow_grid_is_the_l1_path():
+    f = _flow((20, 16, 24), 0.05, 0.1)
+    (a, na), (b, nb) = _both(f, 0.05)[0]
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    assert na == nb
+    assert _both(f, 0.05)[1][1] == 0
