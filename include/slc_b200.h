@@ -128,6 +128,21 @@ SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *v
                           const double *unm1, const double *vnm1, const double *wnm1, double dt,
                           double *ou, double *ov, double *ow, int64_t *nclamp, void *stream);
 
+/* One SL-BDF2 step with its bulk shift (slc_step_bdf2 + slc_bulk_shift) for
+ * a caller whose state lives in HOST memory (page-locked for overlap):
+ * uploads cur = V^n and prev = V^{n-1}, and downloads next = V^{n+1}, p and
+ * bulk_out2 = (u_bulk, forcing).  All are host pointers; the device state is
+ * the library's (double-buffered).  Uploads, compute and downloads overlap:
+ * the copies run on two copy streams in 16 MiB chunks, and an upload whose
+ * host source an earlier call is still downloading into waits for that chunk
+ * only, so feeding each call's next back as the following call's cur
+ * pipelines the round trip.  Returns after enqueueing; the outputs are on the
+ * host, and the host buffers may be touched again, once `stream` completes.
+ * No counterpart in the reference (its state is device- or CPU-resident). */
+SLC_API int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const double *const prev[3],
+                               double *const next[3], double *p, double *bulk_out2, double U_bulk,
+                               double dt, void *stream);
+
 /* slc_trace_gather_bdf2 with each block's two gather source boxes staged
  * in shared memory by the Tensor Memory Accelerator (3-D cp.async.bulk.tensor
  * loads of halo-padded node copies written with U*; FP64 handles with

@@ -64,6 +64,8 @@ SIGNATURES = {
     "slc_departure": ([_P, _I, _P, _P, _P, _D, _P, _P, _P, _P], _I),
     "slc_advect": ([_P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P], _I),
     "slc_trace_gather_bdf2": ([_P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P], _I),
+    "slc_step_bdf2_host": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), _P, _P, _D,
+                            _D, _P], _I),
     "slc_trace_gather_bdf2_staged": ([_P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P], _I),
     "slc_zsolve": ([_P, _P, _P, _P, _D, _P], _I),
     "slc_divergence": ([_P, _P, _P, _P, _P, _P], _I),

@@ -503,6 +503,10 @@ int slc_grid_destroy(slc_grid *g)
     for (cudaEvent_t e : g->evs) cudaEventDestroy(e);
     for (void *p : g->allocs) cudaFree(p);
     if (g->adj) adj_free(g->adj);
+    if (g->host) {
+        cudaDeviceSynchronize();  // copies in flight may still use the host buffers
+        host_step_free(g->host);
+    }
     delete g;
     return SLC_OK;
 }

@@ -12,6 +12,8 @@
 
 struct AdjWS;                 // adjoint workspace (adjoint.cu), allocated on first use
 void adj_free(AdjWS *w);
+struct HostStep;              // host-state step machinery (host_step.cu), on first use
+void host_step_free(HostStep *h);
 
 struct slc_grid {
     SlcParams P{};
@@ -33,6 +35,7 @@ struct slc_grid {
     bool mixed_ready = false;
     MixedWS mws{};
     AdjWS *adj = nullptr;
+    HostStep *host = nullptr;
     TmaSL tma{};
     int tma_state = 0;        // 0 not tried, 1 ready, -1 unavailable (L1 gather path)
     unsigned long long *dev_flags = nullptr;  // staged-gather statistics (launch_sl_tma)
