@@ -58,6 +58,15 @@ def parse_args():
     ap.add_argument("--ensemble-n", type=int, default=48)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout check")
     ap.add_argument("--adjoint-fd-dirs", type=int, default=16)
+    ap.add_argument("--mixed-report", action="store_true",
+                    help="instead of the bench line: the mixed form against the FP64 form over "
+                         "--report-steps steps on --report-grid (JSON lines)")
+    ap.add_argument("--report-grid", type=int, nargs=3, default=[512, 384, 384])
+    ap.add_argument("--report-steps", type=int, default=1000)
+    ap.add_argument("--report-every", type=int, default=100)
+    ap.add_argument("--report-re", type=float, default=2800.0, help="Re key (nu = 1/Re)")
+    ap.add_argument("--report-dt", type=float, default=0.005)
+    ap.add_argument("--report-urms", type=float, default=0.12)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0,
                     help="CPU seconds the cpu_baseline sample aims for")
     return ap.parse_args()
@@ -551,6 +560,75 @@ def measure_adjoint(n_dirs):
     return out
 
 
+def plane_stats(flow):
+    """Plane-averaged U and the rms / uw profiles of the interior fields
+    (u, v at centres; w averaged to centres)."""
+    nx, ny, nz = flow.nx, flow.ny, flow.nz
+    u = flow.u[1:nx + 1, 1:ny + 1, 1:nz + 1]
+    v = flow.v[1:nx + 1, 1:ny + 1, 1:nz + 1]
+    w = 0.5 * (flow.w[1:nx + 1, 1:ny + 1, 0:nz] + flow.w[1:nx + 1, 1:ny + 1, 1:nz + 1])
+    U = u.mean(dim=(0, 1))
+    up, vp, wp = u - U, v - v.mean(dim=(0, 1)), w - w.mean(dim=(0, 1))
+    return {"U": U, "urms": up.pow(2).mean((0, 1)).sqrt(), "vrms": vp.pow(2).mean((0, 1)).sqrt(),
+            "wrms": wp.pow(2).mean((0, 1)).sqrt(), "uw": (up * wp).mean((0, 1))}
+
+
+def run_mixed_report(args):
+    """The mixed form and the FP64 form free-running side by side from one
+    seeded initial field (both with their own BDF1 bootstrap); every
+    `report_every` steps one JSON line with the mixed form's relative
+    velocity errors (L2 and Linf over the three components), its max|div|
+    and bulk velocity, and the drift of its plane-averaged U, u'_rms, v'_rms,
+    w'_rms and uw profiles (max relative difference to the FP64 profiles)."""
+    import torch
+
+    from slchannel_b200.fields import synthetic_channel_field
+    from slchannel_b200.solver import SLChannelFlow
+    from slchannel_b200.utils import compute_bulk_velocity, compute_divergence
+
+    nx, ny, nz = args.report_grid
+    cfg = lambda prec: {  # noqa: E731
+        "grid": {"nx": nx, "ny": ny, "nz": nz},
+        "domain": {"Lx": LX, "Ly": LY, "Lz": LZ, "stretching_type": "symmetric"},
+        "flow": {"Re": args.report_re, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": GAMMA},
+        "initialization": {"type": "parabolic"}, "time": {"dt": args.report_dt},
+        "compute": {"device": "cuda"},
+        "sl": {"interp_order": 6, "n_traj_iters": 2, "interp_dtype": prec}}
+    f64 = SLChannelFlow(config=cfg("fp64"))
+    u, v, w = synthetic_channel_field(nx, ny, nz, LX, LY, LZ, f64.z_f.cpu().numpy(),
+                                      f64.z_c.cpu().numpy(), urms=args.report_urms, seed=12)
+    f64.set_state(*(torch.from_numpy(a) for a in (u, v, w)))
+    f64.apply_bc_uvw()
+    f64.u *= 1.0 / float(compute_bulk_velocity(f64.u, f64.cell_vol_ratio, f64.total_volume))
+    f64._save_and_project_initial()
+    f32 = SLChannelFlow(config=cfg("mixed"))
+    f32.set_state(f64.u, f64.v, f64.w, f64.p)
+    print(json.dumps({"report": "mixed vs FP64", "grid": [nx, ny, nz], "Lx": LX, "Ly": LY,
+                      "nu": 1.0 / args.report_re, "dt": args.report_dt, "urms": args.report_urms,
+                      "order": 6, "steps": args.report_steps}), flush=True)
+    t0 = time.time()
+    for n in range(1, args.report_steps + 1):
+        f64.step_sl_bdf2(args.report_dt)
+        ub32, _ = f32.step_sl_bdf2(args.report_dt)
+        if n % args.report_every and n != args.report_steps:
+            continue
+        num2 = den2 = 0.0
+        linf = 0.0
+        for c in "uvw":
+            a, b = getattr(f32, c), getattr(f64, c)
+            d = a - b
+            num2 += float((d * d).sum())
+            den2 += float((b * b).sum())
+            linf = max(linf, float(d.abs().max() / b.abs().max()))
+        s32, s64 = plane_stats(f32), plane_stats(f64)
+        drift = {k: float((s32[k] - s64[k]).abs().max() / (s64[k].abs().max() or 1.0)) for k in s64}
+        div = compute_divergence(f32.u, f32.v, f32.w, nx, ny, nz, f32.dx, f32.dy, f32.dz_f)
+        print(json.dumps({"step": n, "rel_l2": math.sqrt(num2 / den2), "rel_linf": linf,
+                          "max_div_mixed": float(div.abs().max()), "u_bulk_mixed": float(ub32),
+                          "stats_drift": drift, "wall_s": time.time() - t0}), flush=True)
+    return 0
+
+
 def run_b200(args):
     import torch
 
@@ -721,6 +799,8 @@ def main():
     MIXED_ERROR_STEPS = args.mixed_error_steps
     if args.impl == "reference":
         return run_reference(args)
+    if args.mixed_report:
+        return run_mixed_report(args)
     return run_b200(args)
 
 

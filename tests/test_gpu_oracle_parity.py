@@ -97,10 +97,11 @@ def test_parity_staged_gather_wide_feet():
 
 
 def test_parity_config1_64cubed_20_steps():
-    """Config 1: 64^3 in 2pi x pi x 2, gamma 2, Re_b 2800, order 6, dt 0.01,
-    20 steps (BDF1 bootstrap + 19 BDF2), free-running, against the oracle
-    every step."""
-    run_parity(64, 64, 64, 2 * math.pi, math.pi, 6, steps=20, dt=0.01, urms=0.1, resync=False)
+    """Config 1: 64^3 in 2pi x pi x 2, gamma 2, Re_b 2800 on the channel
+    height (nu = 1/1400), order 6, dt 0.01, 20 steps (BDF1 bootstrap + 19
+    BDF2), free-running, against the oracle every step."""
+    run_parity(64, 64, 64, 2 * math.pi, math.pi, 6, steps=20, dt=0.01, urms=0.1, resync=False,
+               Re=1400.0)
 
 
 def test_parity_large_dt_clamps():
