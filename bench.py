@@ -446,7 +446,7 @@ def measure_mixed(flow64, n, order, K, W, dist):
             "form": "FP32 fluctuation about FP64 plane means in trace+gather; rest FP64"}
 
 
-def measure_ensemble(n_inst, K):
+def measure_ensemble(n_inst, K, precision="fp64"):
     """The ensemble form: n_inst seeded channels (per-axis sizes from
     {32, 48, 64, 96, 128}, gamma in [1.6, 2.2], Re_b in [2000, 5000], dt at
     trajectory CFL 3, order 6, FP64) advanced by one CUDA-graph step, against
@@ -458,7 +458,7 @@ def measure_ensemble(n_inst, K):
     specs = ensemble_specs(n_inst, seed=4)
     flows, dts = [], []
     for s in specs:
-        f, dt = make_flow(s, order=6)
+        f, dt = make_flow(s, order=6, precision=precision)
         f.step_sl_bdf2(dt)
         flows.append(f)
         dts.append(dt)
@@ -489,7 +489,7 @@ def measure_ensemble(n_inst, K):
            "loop_ms_per_step": ms_loop, "speedup_vs_loop": ms_loop / ms_graph,
            "autotuned_tile_z_extents": tiles,
            "workload": f"{n_inst} channels, sizes from {{32,48,64,96,128}} per axis, 2pi x pi x 2, "
-                       "gamma U[1.6,2.2], Re_b U[2000,5000], dt at trajectory CFL 3, order 6, FP64"}
+                       f"gamma U[1.6,2.2], Re_b U[2000,5000], dt at trajectory CFL 3, order 6, {precision}"}
     ens.close()
     del flows, ens
     torch.cuda.empty_cache()
@@ -779,6 +779,7 @@ def run_b200(args):
     }
     if world == 1 and not args.no_ensemble:
         line["ensemble"] = measure_ensemble(args.ensemble_n, K)
+        line["ensemble_mixed"] = measure_ensemble(args.ensemble_n, K, "mixed")
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = measure_adjoint(args.adjoint_fd_dirs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -313,12 +313,12 @@ SLC_API int slc_adjoint_step(slc_grid *g, int mode, double *const cur[3], double
  *    (nx, ny);
  *  - the step can be captured once per phase into a CUDA graph.
  * Per instance the arithmetic is that of slc_step_bdf2 followed by
- * slc_bulk_shift, so an instance matches the same channel stepped alone.
- * FP64 form only. */
+ * slc_bulk_shift, so an instance matches the same channel stepped alone, in
+ * the FP64 or (all instances alike) the mixed form. */
 typedef struct slc_ensemble slc_ensemble; /* opaque */
 
-/* n instances; descs[i] as for slc_grid_create (one order, one device,
- * precision SLC_PREC_FP64, nz >= 2).  Synchronous. */
+/* n instances; descs[i] as for slc_grid_create (one order, one device, one
+ * precision, nz >= 2).  Synchronous. */
 SLC_API int slc_ensemble_create(const slc_grid_desc *descs, int n, slc_ensemble **out);
 SLC_API int slc_ensemble_destroy(slc_ensemble *e);
 SLC_API int slc_ensemble_size(const slc_ensemble *e);

@@ -23,6 +23,7 @@
 struct slc_ensemble {
     int device = 0;
     int order = 6;
+    int mixed = 0;  // all instances in the mixed form
     std::vector<slc_grid *> grids;
     std::vector<EnsInst> host_inst;
     std::vector<int> tkl;
@@ -37,7 +38,7 @@ struct slc_ensemble {
     // item ranges inside d_items
     struct Range {
         int off = 0, n = 0;
-    } r_bc, r_lin, r_sl, r_zs, r_div, r_th, r_pr, r_bulk;
+    } r_bc, r_lin, r_sl, r_zs, r_div, r_th, r_pr, r_bulk, r_pp, r_pack;
     int max_ch = 1;
     int sl_grid = 148;
     // FFT groups (instances sharing nx, ny): pools and plans
@@ -202,6 +203,24 @@ void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
     for (int i = 0; i < n; ++i)
         for (int b = 0; b < kBulkBlocks; ++b) items.push_back({i, b, 0, 0});
     end(e->r_bulk);
+    // mixed form: plane-mean partials (column group, field) and FP32 packs
+    begin(e->r_pp);
+    if (e->mixed)
+        for (int i = 0; i < n; ++i)
+            for (int f = 0; f < 6; ++f)
+                for (int b = 0; b < mixed_mean_blocks(); ++b) items.push_back({i, b, f, 0});
+    end(e->r_pp);
+    begin(e->r_pack);
+    if (e->mixed)
+        for (int i = 0; i < n; ++i) {
+            const SlcParams &P = e->grids[i]->P;
+            const MixedWS &ws = e->grids[i]->mws;
+            const int nzp = std::max(ws.nzp[0], ws.nzp[2]);
+            for (int z = 0; z < 3 * P.nx; ++z)
+                for (int y = 0; y < P.ny; ++y)
+                    for (int x = 0; x < (nzp + 127) / 128; ++x) items.push_back({i, x, y, z});
+        }
+    end(e->r_pack);
 }
 
 int upload_tables(slc_ensemble *e)
@@ -236,12 +255,22 @@ int enqueue_step(slc_ensemble *e, int ph, cudaStream_t s)
     const int cur = ens_cur(ph), nxt = ens_next(ph);
     const EnsInst *I = e->d_inst;
     ENS_CK(launch_bc_ens(I, items_at(e, e->r_bc), e->r_bc.n, cur, 0, s), "boundary conditions");
-    ENS_CK(launch_lincomb_ens(I, items_at(e, e->r_lin), e->r_lin.n, ph, s), "U* = 2V^n - V^{n-1}");
+    if (e->mixed)
+        ENS_CK(launch_mixed_prepare_ens(I, n, items_at(e, e->r_pp), e->r_pp.n, items_at(e, e->r_pack),
+                                        e->r_pack.n, ph, s),
+               "mixed-form means and packs");
+    else
+        ENS_CK(launch_lincomb_ens(I, items_at(e, e->r_lin), e->r_lin.n, ph, s), "U* = 2V^n - V^{n-1}");
     for (int i = 0; i < n; ++i)
         ENS_CK(cudaMemsetAsync(e->host_inst[i].ncl, 0, sizeof(unsigned long long), s), "memset");
     ENS_CK(cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned), s), "memset");
-    ENS_CK(launch_sl_ens(I, items_at(e, e->r_sl), e->r_sl.n, ph, e->order, e->d_queue, e->sl_grid, s),
-           "trace+gather BDF2");
+    if (e->mixed)
+        ENS_CK(launch_sl_mixed_ens(I, items_at(e, e->r_sl), e->r_sl.n, ph, e->order, e->d_queue,
+                                   e->sl_grid, s),
+               "mixed trace+gather BDF2");
+    else
+        ENS_CK(launch_sl_ens(I, items_at(e, e->r_sl), e->r_sl.n, ph, e->order, e->d_queue, e->sl_grid, s),
+               "trace+gather BDF2");
     ENS_CK(launch_zsolve_ens(I, items_at(e, e->r_zs), e->r_zs.n, nxt, e->max_ch, s), "z-solve");
     ENS_CK(launch_div_pack_ens(I, items_at(e, e->r_div), e->r_div.n, nxt, s), "divergence");
     for (auto &gr : e->groups) {
@@ -277,8 +306,8 @@ int slc_ensemble_create(const slc_grid_desc *descs, int n, slc_ensemble **out)
     if (!descs || !out || n < 1) return efail(nullptr, SLC_E_INVALID, "need descriptors, n >= 1 and an output pointer");
     *out = nullptr;
     for (int i = 0; i < n; ++i) {
-        if (descs[i].precision != SLC_PREC_FP64)
-            return efail(nullptr, SLC_E_INVALID, "the ensemble step runs the FP64 form only");
+        if (descs[i].precision != descs[0].precision)
+            return efail(nullptr, SLC_E_INVALID, "all instances of an ensemble share one precision");
         if (descs[i].order != descs[0].order)
             return efail(nullptr, SLC_E_INVALID, "all instances of an ensemble share one interp_order");
         if (descs[i].device != descs[0].device)
@@ -289,6 +318,7 @@ int slc_ensemble_create(const slc_grid_desc *descs, int n, slc_ensemble **out)
     slc_ensemble *e = new slc_ensemble();
     e->device = descs[0].device;
     e->order = descs[0].order;
+    e->mixed = descs[0].precision == SLC_PREC_MIXED ? 1 : 0;
     DevGuard dg(e->device);
     for (int i = 0; i < n; ++i) {
         slc_grid *g = nullptr;
@@ -444,6 +474,12 @@ int slc_ensemble_bind(slc_ensemble *e, double *const *lev, double *const *p, con
         I.Ly = g->Ly;
         I.U_bulk = U_bulk[i];
         I.tkl = e->tkl[i];
+        if (e->mixed) {
+            int rm = slc_grid_ensure_mixed(g);
+            if (rm) return efail(e, rm, std::string("instance ") + std::to_string(i) + ": " + g->err);
+            I.mixed = 1;
+            I.mws = g->mws;
+        }
     }
     ENS_CK(cudaDeviceSynchronize(), "z-solve tables");
     int rc = upload_tables(e);
@@ -513,7 +549,12 @@ int slc_ensemble_autotune(slc_ensemble *e, int phase, int reps, int *tkl_out, do
     cudaStream_t s = (cudaStream_t)stream;
     const int n = (int)e->grids.size();
     ENS_CK(launch_bc_ens(e->d_inst, items_at(e, e->r_bc), e->r_bc.n, ens_cur(phase), 0, s), "bc");
-    ENS_CK(launch_lincomb_ens(e->d_inst, items_at(e, e->r_lin), e->r_lin.n, phase, s), "U*");
+    if (e->mixed)
+        ENS_CK(launch_mixed_prepare_ens(e->d_inst, n, items_at(e, e->r_pp), e->r_pp.n, items_at(e, e->r_pack),
+                                        e->r_pack.n, phase, s),
+               "mixed prepare");
+    else
+        ENS_CK(launch_lincomb_ens(e->d_inst, items_at(e, e->r_lin), e->r_lin.n, phase, s), "U*");
     std::map<std::vector<int>, std::vector<int>> shapes;
     for (int i = 0; i < n; ++i) {
         const SlcParams &P = e->grids[i]->P;
@@ -553,8 +594,10 @@ int slc_ensemble_autotune(slc_ensemble *e, int phase, int reps, int *tkl_out, do
                 ce = cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned), s);
                 if (ce == cudaSuccess && r == 1) ce = cudaEventRecord(a, s);
                 if (ce == cudaSuccess)
-                    ce = launch_sl_ens(e->d_inst, d_tmp, (int)items.size(), phase, e->order, e->d_queue,
-                                       e->sl_grid, s);
+                    ce = e->mixed ? launch_sl_mixed_ens(e->d_inst, d_tmp, (int)items.size(), phase, e->order,
+                                                        e->d_queue, e->sl_grid, s)
+                                  : launch_sl_ens(e->d_inst, d_tmp, (int)items.size(), phase, e->order,
+                                                  e->d_queue, e->sl_grid, s);
             }
             if (ce == cudaSuccess) ce = cudaEventRecord(b, s);
             if (ce == cudaSuccess) ce = cudaEventSynchronize(b);

@@ -271,16 +271,13 @@ __device__ __forceinline__ double xy_diffusion64(const SlcParams &P, const doubl
 // FA/FB: the mixed views of the near (V^n) and far (V^{n-1}) fields of
 // component C; fn/fnm1: the same fields in FP64 (ghost-shaped) for R.
 template <int C, int O, int MODE>
-__global__ void __launch_bounds__(kThreads, 2)
-    k_sl_mixed(SlcParams P, Vel3M M, MixedView FA, MixedView FB, const double *__restrict__ fn,
-               const double *__restrict__ fnm1, double dt, double *__restrict__ out,
-               unsigned long long *nclamp)
+__device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &M, const MixedView &FA,
+                                               const MixedView &FB, const double *__restrict__ fn,
+                                               const double *__restrict__ fnm1, double dt,
+                                               double *__restrict__ out, int i, int j, int k,
+                                               unsigned &ncl)
 {
     const int nzi = (C == 2) ? P.nz - 1 : P.nz;
-    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
-    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
-    const int i = blockIdx.z;
-    unsigned ncl = 0;
     if (k < nzi && j < P.ny) {
         const Arr32 A = arrival32<C>(P, i, j, k);
         double u0, v0, w0;
@@ -305,6 +302,19 @@ __global__ void __launch_bounds__(kThreads, 2)
         const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
         out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
     }
+}
+
+template <int C, int O, int MODE>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_sl_mixed(SlcParams P, Vel3M M, MixedView FA, MixedView FB, const double *__restrict__ fn,
+               const double *__restrict__ fnm1, double dt, double *__restrict__ out,
+               unsigned long long *nclamp)
+{
+    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
+    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
+    const int i = blockIdx.z;
+    unsigned ncl = 0;
+    sl_point_mixed<C, O, MODE>(P, M, FA, FB, fn, fnm1, dt, out, i, j, k, ncl);
     add_clamps(nclamp, ncl);
 }
 
@@ -317,13 +327,11 @@ struct MeanSrcs {
     int comp[9];
 };
 
-__global__ void __launch_bounds__(256) k_plane_partials(SlcParams P, MeanSrcs S, double *partials,
-                                                        int ldp)
+__device__ __forceinline__ void plane_partial(const SlcParams &P, const double *src, int C,
+                                              double *partials, int ldp, int f, int b, int G)
 {
-    const int f = blockIdx.y, b = blockIdx.x, G = gridDim.x;
-    const int C = S.comp[f];
     const int NZ = C == 2 ? P.nz + 1 : P.nz + 2;
-    const NodeView<double> V = ghost_view<double>(C, S.p[f], P.nx, P.ny, P.nz);
+    const NodeView<double> V = ghost_view<double>(C, src, P.nx, P.ny, P.nz);
     constexpr int kMaxPer = 5;  // NZ <= 1026 levels over 256 threads
     double acc[kMaxPer];
 #pragma unroll
@@ -346,6 +354,13 @@ __global__ void __launch_bounds__(256) k_plane_partials(SlcParams P, MeanSrcs S,
     }
 }
 
+__global__ void __launch_bounds__(256) k_plane_partials(SlcParams P, MeanSrcs S, double *partials,
+                                                        int ldp)
+{
+    const int f = blockIdx.y;
+    plane_partial(P, S.p[f], S.comp[f], partials, ldp, f, blockIdx.x, gridDim.x);
+}
+
 // means[f][k] = sum_b partials / (nx ny); with derived_star, fields 6..8 (U*)
 // are 2 mean(A) - mean(B) instead of summed.
 struct MeanPtrs {
@@ -353,10 +368,10 @@ struct MeanPtrs {
     float *m32[9];
 };
 
-__global__ void k_plane_finish(SlcParams P, int nf, const double *partials, int ldp, int G,
-                               MeanPtrs out, int derived_star)
+__device__ __forceinline__ void plane_finish(const SlcParams &P, int nf, const double *partials,
+                                             int ldp, int G, const MeanPtrs &out, int derived_star,
+                                             int f)
 {
-    const int f = blockIdx.x;
     const int NZ = (f % 3) == 2 ? P.nz + 1 : P.nz + 2;
     const double inv = 1.0 / ((double)P.nx * (double)P.ny);
     for (int k = threadIdx.x; k < NZ; k += blockDim.x) {
@@ -379,6 +394,12 @@ __global__ void k_plane_finish(SlcParams P, int nf, const double *partials, int 
     }
 }
 
+__global__ void k_plane_finish(SlcParams P, int nf, const double *partials, int ldp, int G,
+                               MeanPtrs out, int derived_star)
+{
+    plane_finish(P, nf, partials, ldp, G, out, derived_star, blockIdx.x);
+}
+
 // FP32 fluctuation node buffers: field slot q = comp (0..2) + 3 * which
 // (0 A, 1 B, 2 U*), U* = M or 2A - B.
 struct PackArgs {
@@ -388,11 +409,12 @@ struct PackArgs {
     int nzp[3];
 };
 
-__global__ void __launch_bounds__(128) k_pack_mixed(SlcParams P, PackArgs a)
+__device__ __forceinline__ void pack_mixed(const SlcParams &P, const PackArgs &a, int bx, int by,
+                                           int bz)
 {
-    const int comp = blockIdx.z / P.nx, i = blockIdx.z - comp * P.nx;
-    const int j = blockIdx.y;
-    const int k = blockIdx.x * 128 + threadIdx.x;
+    const int comp = bz / P.nx, i = bz - comp * P.nx;
+    const int j = by;
+    const int k = bx * 128 + threadIdx.x;
     const int NZ = comp == 2 ? P.nz + 1 : P.nz + 2;
     const int NZp = a.nzp[comp];
     if (k >= NZp) return;
@@ -417,6 +439,108 @@ __global__ void __launch_bounds__(128) k_pack_mixed(SlcParams P, PackArgs a)
     a.f32[comp][o] = (float)(va - a.mean[comp][k]);
     a.f32[comp + 3][o] = (float)(vb - a.mean[comp + 3][k]);
     a.f32[comp + 6][o] = (float)(vm - a.mean[comp + 6][k]);
+}
+
+__global__ void __launch_bounds__(128) k_pack_mixed(SlcParams P, PackArgs a)
+{
+    pack_mixed(P, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---- ensemble forms (one launch per substep over all instances) ----
+__device__ __forceinline__ MixedView mview_dev(const MixedWS &ws, int slot, const SlcParams &P)
+{
+    MixedView v;
+    const int comp = slot % 3;
+    v.f = node_view<float>(ws.f32[slot], P.ny, ws.nzp[comp]);
+    v.mean = ws.mean[slot];
+    v.mean32 = ws.mean32[slot];
+    return v;
+}
+
+// items (inst, column group b, field f): f < 3 the near field V^n, else V^{n-1}
+__global__ void __launch_bounds__(256) k_plane_partials_ens(const EnsInst *__restrict__ ins,
+                                                            const EnsItem *__restrict__ items, int ph)
+{
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    const int f = it.b;
+    const double *src = f < 3 ? I.lev[ens_cur(ph)][f] : I.lev[ens_prev(ph)][f - 3];
+    plane_partial(I.P, src, f % 3, I.mws.partials, I.P.nz + 2, f, it.a, kMeanBlocks);
+}
+
+// block (inst * 9 + f)
+__global__ void k_plane_finish_ens(const EnsInst *__restrict__ ins)
+{
+    const EnsInst &I = ins[blockIdx.x / 9];
+    const int f = blockIdx.x % 9;
+    MeanPtrs mp;
+    for (int q = 0; q < 9; ++q) {
+        mp.m[q] = I.mws.mean[q];
+        mp.m32[q] = I.mws.mean32[q];
+    }
+    plane_finish(I.P, 6, I.mws.partials, I.P.nz + 2, kMeanBlocks, mp, 1, f);
+}
+
+// items (inst, bx, by, bz) as k_pack_mixed's grid
+__global__ void __launch_bounds__(128) k_pack_mixed_ens(const EnsInst *__restrict__ ins,
+                                                        const EnsItem *__restrict__ items, int ph)
+{
+    const EnsItem it = items[blockIdx.x];
+    const EnsInst &I = ins[it.inst];
+    PackArgs a;
+    for (int c = 0; c < 3; ++c) {
+        a.A[c] = I.lev[ens_cur(ph)][c];
+        a.B[c] = I.lev[ens_prev(ph)][c];
+        a.M[c] = nullptr;
+        a.nzp[c] = I.mws.nzp[c];
+    }
+    for (int q = 0; q < 9; ++q) {
+        a.f32[q] = I.mws.f32[q];
+        a.mean[q] = I.mws.mean[q];
+    }
+    pack_mixed(I.P, a, it.a, it.b, it.c);
+}
+
+// Persistent mixed-form BDF2 trace+gather over the (instance, component, x
+// index, tile) queue; the structure of the FP64 ensemble kernel.
+template <int O>
+__global__ void __launch_bounds__(kThreads, 2) k_sl_mixed_ens(const EnsInst *__restrict__ ins,
+                                                              const EnsItem *__restrict__ items,
+                                                              int nitems, int ph, unsigned *queue)
+{
+    __shared__ SlcParams sP;
+    __shared__ int s_item;
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+    int have = -1;
+    for (;;) {
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const EnsItem w = items[it];
+        if (w.inst != have) {
+            const unsigned long long *src = (const unsigned long long *)&ins[w.inst].P;
+            unsigned long long *dst = (unsigned long long *)&sP;
+            for (int q = threadIdx.x; q < (int)(sizeof(SlcParams) / 8); q += kThreads) dst[q] = src[q];
+            have = w.inst;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+        const EnsInst &I = ins[w.inst];
+        const int tkl = I.tkl;
+        const int k = ((w.c & 0xffff) << tkl) + (threadIdx.x & ((1 << tkl) - 1));
+        const int j = ((w.c >> 16) << (8 - tkl)) + (threadIdx.x >> tkl);
+        const int i = w.b;
+        const Vel3M M{mview_dev(I.mws, 6, sP), mview_dev(I.mws, 7, sP), mview_dev(I.mws, 8, sP)};
+        const MixedView FA = mview_dev(I.mws, w.a, sP), FB = mview_dev(I.mws, w.a + 3, sP);
+        const double *fn = I.lev[ens_cur(ph)][w.a];
+        const double *fnm1 = I.lev[ens_prev(ph)][w.a];
+        double *out = I.lev[ens_next(ph)][w.a];
+        unsigned ncl = 0;
+        if (w.a == 0) sl_point_mixed<0, O, 2>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else if (w.a == 1) sl_point_mixed<1, O, 2>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else sl_point_mixed<2, O, 2>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
+        add_clamps(I.ncl, ncl);
+    }
 }
 
 MixedView mview(const MixedWS &ws, int slot, const SlcParams &P)
@@ -499,5 +623,28 @@ cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, cons
         else if (mode == 1) launch_t<6, 1>(P, fn, fnm1, ws, dt, out, nclamp, s);
         else launch_t<6, 2>(P, fn, fnm1, ws, dt, out, nclamp, s);
     }
+    return cudaGetLastError();
+}
+
+int mixed_mean_blocks() { return kMeanBlocks; }
+
+cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsItem *pp_items, int n_pp,
+                                     const EnsItem *pack_items, int n_pack, int ph, cudaStream_t s)
+{
+    if (ninst <= 0) return cudaSuccess;
+    k_plane_partials_ens<<<n_pp, 256, 0, s>>>(ins, pp_items, ph);
+    k_plane_finish_ens<<<9 * ninst, 256, 0, s>>>(ins);
+    k_pack_mixed_ens<<<n_pack, 128, 0, s>>>(ins, pack_items, ph);
+    count_launches(3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sl_mixed_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
+                                unsigned *queue, int grid, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    if (order == 4) k_sl_mixed_ens<4><<<grid, kThreads, 0, s>>>(ins, items, nitems, ph, queue);
+    else k_sl_mixed_ens<6><<<grid, kThreads, 0, s>>>(ins, items, nitems, ph, queue);
+    count_launches(1);
     return cudaGetLastError();
 }

@@ -193,6 +193,12 @@ int ensure_mixed(slc_grid *g)
     return SLC_OK;
 }
 
+}  // namespace
+
+int slc_grid_ensure_mixed(slc_grid *g) { return ensure_mixed(g); }
+
+namespace {
+
 unsigned long long *counter(slc_grid *g, int64_t *user)
 {
     return user ? (unsigned long long *)user : g->ncl_scratch;

@@ -51,3 +51,5 @@ struct slc_grid {
     size_t ev_used = 0;
 };
 
+// Allocate the mixed form's workspace of a mixed-precision handle (slc_api.cu).
+int slc_grid_ensure_mixed(slc_grid *g);

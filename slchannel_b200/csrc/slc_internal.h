@@ -119,6 +119,8 @@ struct EnsInst {
     double *bulk_out;               // [u_bulk after the shift, forcing]
     double dt, Lx, Ly, U_bulk;
     int tkl;                        // SL tile: 2^tkl z points x 2^(8 - tkl) y rows
+    int mixed;                      // mixed form: mws holds the FP32 workspace
+    MixedWS mws;
 };
 // A block's work: instance and three kernel-specific coordinates.
 struct EnsItem {
@@ -174,3 +176,13 @@ cudaError_t launch_mid_pack(const SlcParams &P, Tri cur, Tri prev, TriMut mid, c
 cudaError_t launch_sl_tma(const SlcParams &P, Tri fn, Tri fnm1, Tri mid, double dt, TriMut out,
                           unsigned long long *nclamp, unsigned long long *stats, const TmaSL &T,
                           cudaStream_t s);
+
+// sl_mixed.cu, ensemble forms of the mixed predictor: plane means of V^n and
+// V^{n-1} (items (inst, column group, field 0..5)), their finish, the FP32
+// packs (items (inst, bx, by, bz) of k_pack_mixed's grid), and the
+// persistent trace+gather.
+int mixed_mean_blocks();
+cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsItem *pp_items, int n_pp,
+                                     const EnsItem *pack_items, int n_pack, int ph, cudaStream_t s);
+cudaError_t launch_sl_mixed_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
+                                unsigned *queue, int grid, cudaStream_t s);

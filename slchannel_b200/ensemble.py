@@ -105,7 +105,7 @@ def _desc(flow, order, keep):
     d.stretching = 0 if flow.stretching_type == "symmetric" else 1
     d.order, d.traj_order, d.n_traj_iters = int(order), 2, int(flow.sl_traj_iters)
     d.top_wall_neumann = 1 if flow.top_wall_bc_type == "neumann" else 0
-    d.precision = N.PREC_FP64
+    d.precision = N.PREC_FP64 if flow.sl_interp_dtype == "fp64" else N.PREC_MIXED
     d.nu = float(flow.nu)
     d.z_f = ctypes.cast(zf.data_ptr(), ctypes.POINTER(ctypes.c_double))
     d.z_c = ctypes.cast(zc.data_ptr(), ctypes.POINTER(ctypes.c_double))
@@ -137,6 +137,8 @@ class ChannelEnsemble:
         order = flows[0].sl_order
         if any(f.sl_order != order for f in flows):
             raise ValueError("all instances of an ensemble share one interp_order")
+        if any((f.sl_interp_dtype == "fp64") != (flows[0].sl_interp_dtype == "fp64") for f in flows):
+            raise ValueError("all instances of an ensemble share one precision form")
         if any(f.u_nm1 is None for f in flows):
             raise ValueError("every flow must have taken its BDF1 bootstrap step")
         L = N.lib()

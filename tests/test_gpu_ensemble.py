@@ -33,10 +33,10 @@ def _specs():
     return out
 
 
-def _bootstrapped(specs):
+def _bootstrapped(specs, precision="fp64"):
     flows, dts = [], []
     for s in specs:
-        f, dt = make_flow(s, order=6)
+        f, dt = make_flow(s, order=6, precision=precision)
         f.step_sl_bdf2(dt)  # BDF1 bootstrap
         flows.append(f)
         dts.append(dt)
@@ -47,11 +47,11 @@ def _rel(a, b):
     return ((a - b).abs().max() / b.abs().max()).item()
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_ensemble_matches_single_channel_loop(use_graph):
+@pytest.mark.parametrize("use_graph,precision", [(True, "fp64"), (False, "fp64"), (True, "mixed")])
+def test_ensemble_matches_single_channel_loop(use_graph, precision):
     specs = _specs()
-    ref, dts = _bootstrapped(specs)
-    mine, dts2 = _bootstrapped(specs)
+    ref, dts = _bootstrapped(specs, precision)
+    mine, dts2 = _bootstrapped(specs, precision)
     assert dts == dts2
     ens = ChannelEnsemble(mine, dts, use_graph=use_graph, autotune=False)
     worst = 0.0
@@ -69,7 +69,7 @@ def test_ensemble_matches_single_channel_loop(use_graph):
             assert abs(float(fc) - float(f.forcing)) <= 1e-12 * max(1.0, abs(float(f.forcing)))
             assert int(ens.nclamp[i]) == int(f.sl.n_clamped_last)
             assert _rel(ens.p[i], f.p) <= 1e-12
-    print(f"ensemble vs loop: max relative difference {worst:.3e}")
+    print(f"ensemble vs loop ({precision}): max relative difference {worst:.3e}")
 
 
 def test_ensemble_tiles_do_not_change_results():
@@ -111,6 +111,16 @@ def test_ensemble_specs_recipe():
         assert s["nx"] in (32, 48, 64, 96, 128) and s["nz"] in (32, 48, 64, 96, 128)
         assert 1.6 <= s["gamma"] <= 2.2 and 2000.0 <= s["Re"] <= 5000.0
     assert specs == ensemble_specs(48, seed=4)
+
+
+def test_ensemble_rejects_mixed_precisions():
+    specs = _specs()[:2]
+    f0, d0 = make_flow(specs[0], order=6)
+    f1, d1 = make_flow(specs[1], order=6, precision="mixed")
+    f0.step_sl_bdf2(d0)
+    f1.step_sl_bdf2(d1)
+    with pytest.raises(ValueError):
+        ChannelEnsemble([f0, f1], [d0, d1])
 
 
 def test_ensemble_rejects_mixed_orders():
