@@ -63,9 +63,19 @@ def initialize_flow(nx, ny, nz, z_c, Ly, Lz, U_bulk=1.0, init_type="parabolic",
 
 
 def initialize_flow_from_file(field_file, device="cpu", reset_time=False):
-    """initflow.py:225-286: (u, v, w, p, step, time) from a fields .npz."""
-    d = np.load(field_file)
-    t = lambda k: torch.from_numpy(np.ascontiguousarray(d[k], dtype=np.float64)).to(device)  # noqa: E731
-    step = int(d["step"]) if "step" in d.files and not reset_time else 0
-    time = float(d["time"]) if "time" in d.files and not reset_time else 0.0
-    return t("u"), t("v"), t("w"), t("p"), step, time
+    """initflow.py:225-286: (u, v, w, p, step, time) from a fields .npz
+    written by save_flow_fields; the wall ghosts are re-applied as the
+    reference does (u, v odd at both walls, w = 0 on both walls)."""
+    from .utils import load_flow_fields
+
+    fields = load_flow_fields(field_file, device=device)
+    u, v, w, p = fields["u"], fields["v"], fields["w"], fields["p"]
+    step = 0 if reset_time else int(fields["step"])
+    time = 0.0 if reset_time else float(fields["time"])
+    u[:, :, 0] = -u[:, :, 1]
+    u[:, :, -1] = -u[:, :, -2]
+    v[:, :, 0] = -v[:, :, 1]
+    v[:, :, -1] = -v[:, :, -2]
+    w[:, :, 0] = 0.0
+    w[:, :, -1] = 0.0
+    return u, v, w, p, step, time

@@ -16,6 +16,7 @@ package.
 
 from __future__ import annotations
 
+import numpy as np
 import torch
 import yaml
 
@@ -129,6 +130,11 @@ class SLChannelFlow:
         elif field_file is not None and init_cfg.get("type", "parabolic") != "interpolate":
             self.u, self.v, self.w, self.p, self.initial_step, self.time = initialize_flow_from_file(
                 field_file, device=self.device, reset_time=init_cfg.get("reset_time", False))
+            # the bulk-forcing state saved with the fields (solver.py:338-350)
+            try:
+                self.forcing = float(np.load(field_file)["forcing"])
+            except Exception:
+                self.forcing = 0.0
         else:
             self.u, self.v, self.w, self.p = initialize_flow(
                 self.nx, self.ny, self.nz, self.z_c, self.Ly, self.Lz, U_bulk=self.U_bulk,

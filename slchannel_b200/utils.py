@@ -7,6 +7,7 @@ libslc_b200.so and return device tensors.
 
 from __future__ import annotations
 
+import numpy as np
 import torch
 
 from . import _native as N
@@ -72,3 +73,37 @@ def compute_bulk_velocity(u, cell_vol_ratio, total_volume):
                                        N.stream_of(u))
     N.check(rc)
     return out
+
+
+def save_flow_fields(u, v, w, p, z_c, z_f, Lx, Ly, step, time, u_tau, forcing, results_folder,
+                     filename="fields.npz"):
+    """utils.py:183-214: the reference's checkpoint, one .npz with the
+    ghost-shaped u, v, w, p, the z tables, Lx, Ly, step, time, u_tau and
+    forcing (tensors are copied to the host; scalars stored as 0-d arrays)."""
+    import os
+
+    def host(x):
+        return x.detach().cpu().numpy() if torch.is_tensor(x) else x
+
+    def scalar(x):
+        return x.item() if torch.is_tensor(x) else x
+
+    np.savez(os.path.join(results_folder, filename), u=host(u), v=host(v), w=host(w), p=host(p),
+             z_c=host(z_c), z_f=host(z_f), Lx=Lx, Ly=Ly, step=step, time=time,
+             u_tau=scalar(u_tau), forcing=scalar(forcing))
+
+
+def load_flow_fields(filepath, device="cpu"):
+    """utils.py:216-258: the checkpoint as a dict of tensors (u, v, w, p,
+    z_c, z_f on `device`) and floats / ints (Lx, Ly, step, time, u_tau,
+    forcing).  Raises FileNotFoundError for a missing file."""
+    import os
+
+    if not os.path.exists(filepath):
+        raise FileNotFoundError(f"Field file not found: {filepath}")
+    data = np.load(filepath)
+    t = lambda k: torch.tensor(data[k], device=device)  # noqa: E731
+    return {"u": t("u"), "v": t("v"), "w": t("w"), "p": t("p"), "z_c": t("z_c"), "z_f": t("z_f"),
+            "Lx": float(data["Lx"]), "Ly": float(data["Ly"]), "step": int(data["step"]),
+            "time": float(data["time"]), "u_tau": float(data["u_tau"]),
+            "forcing": float(data["forcing"])}
