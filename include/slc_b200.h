@@ -262,6 +262,17 @@ SLC_API int slc_step_bdf2(slc_grid *g, double *const cur[3], double *const prev[
  * accumulated record.  Adds two cudaEventRecord calls per phase per call. */
 SLC_API int slc_timing(slc_grid *g, int enable);
 
+/* One BDF2 step with the incremental pressure (sl.bdf2_pressure: inc,
+ * solver.py:905-941, 1001-1012), up to the bulk shift.  p_cur holds the full
+ * pressure p^n and p_prev p^{n-1} (have_prev = 0 on the first BDF2 step after
+ * a BDF1 bootstrap, whose p is its phi).  The predictor gets
+ * -(2dt/3) grad(p_ext), p_ext = 2 p^n - p^{n-1} (p^n without a history),
+ * before the z-solve.  On return p_cur = p_ext + phi and p_prev = the old
+ * p_cur.  Ghost-shaped pressures; next's w wall faces must hold 0. */
+SLC_API int slc_step_bdf2_inc(slc_grid *g, double *const cur[3], double *const prev[3],
+                              double *const next[3], double *p_cur, double *p_prev, int have_prev,
+                              double dt, int64_t *nclamp, void *stream);
+
 /* Synchronise on the recorded events and return, per phase, the summed
  * elapsed milliseconds and the number of timed intervals; resets the record.
  * ms and count each hold SLC_NPHASE entries. */

@@ -559,13 +559,13 @@ def project_velocity(u, v, w, p, nx, ny, nz, dx, dy, dz_c, dz_f, dt):
 
 
 class OracleChannel:
-    """State and step of SLChannelFlow's SL-BDF2 scheme (noninc pressure,
-    theta = 1 z-solve, exact bulk shift), on numpy arrays."""
+    """State and step of SLChannelFlow's SL-BDF2 scheme (noninc or inc
+    pressure, theta = 1 z-solve, exact bulk shift), on numpy arrays."""
 
     def __init__(self, nx, ny, nz, Lx, Ly, Lz, gamma, nu, u, v, w, p=None, *,
                  stretching_type="symmetric", order=6, traj_order=2, n_traj_iters=2,
                  top_wall_bc_type="dirichlet", U_bulk=1.0, xy_rhs="extrap",
-                 z_f=None, z_c=None, bulk_forcing=True):
+                 z_f=None, z_c=None, bulk_forcing=True, bdf2_pressure="noninc"):
         self.nx, self.ny, self.nz = nx, ny, nz
         self.Lx, self.Ly, self.Lz = Lx, Ly, Lz
         self.dx, self.dy = Lx / nx, Ly / ny
@@ -590,6 +590,8 @@ class OracleChannel:
         self.dt_prev = None
         self.n_clamped_last = 0
         self.forcing = 0.0
+        self.pressure = bdf2_pressure
+        self.P_curr = self.P_prev = None  # full pressure levels of the inc branch
 
     def apply_bc(self):
         apply_bc_all(self.u, self.v, self.w, self.top)
@@ -635,6 +637,7 @@ class OracleChannel:
                          self.dy, self.dz_c, self.dz_f, dt_proj)
         self.p = phi
         self.apply_bc()
+        return phi
 
     def _bulk_shift(self, dt):
         """solver.py:694-723 -- exact uniform shift of u to the target bulk."""
@@ -672,7 +675,10 @@ class OracleChannel:
         self._zsolve_all(dt)
         if cap is not None:
             cap["zsolve"] = (self.u.copy(), self.v.copy(), self.w.copy())
-        self._project(dt, dt, cap)
+        phi = self._project(dt, dt, cap)
+        if self.pressure == "inc":  # solver.py:802-807
+            self.P_curr = phi.copy()
+            self.P_prev = None
         if cap is not None:
             cap["proj"] = (self.u.copy(), self.v.copy(), self.w.copy())
         self.dt_prev = dt
@@ -680,7 +686,7 @@ class OracleChannel:
         return (ub, f, cap) if capture else (ub, f)
 
     def step_bdf2(self, dt, capture=False):
-        """solver.py:813-1018 (noninc pressure)."""
+        """solver.py:813-1018 (noninc or inc pressure)."""
         nx, ny, nz = self.nx, self.ny, self.nz
         self.apply_bc()
         if self.u_nm1 is None or self.dt_prev is None or abs(dt - self.dt_prev) > 1e-12 * dt:
@@ -703,6 +709,14 @@ class OracleChannel:
         dt_eff = (2.0 / 3.0) * dt
         outs = [n * (4.0 / 3.0) + f * (-1.0 / 3.0) for n, f in zip(near, far)]
         self._interior_add(outs, Rh, dt_eff)
+        p_ext = None
+        if self.pressure == "inc" and self.P_curr is not None:  # solver.py:905-941
+            p_ext = self.P_curr if self.P_prev is None else 2.0 * self.P_curr - self.P_prev
+            gp = [np.zeros_like(o) for o in outs]
+            project_velocity(gp[0], gp[1], gp[2], p_ext, nx, ny, nz, self.dx, self.dy,
+                             self.dz_c, self.dz_f, 1.0)
+            for o, g in zip(outs, gp):
+                o += dt_eff * g
         self.u_nm1, self.v_nm1, self.w_nm1 = self.u.copy(), self.v.copy(), self.w.copy()
         self.u, self.v, self.w = outs
         self.apply_bc()
@@ -711,7 +725,17 @@ class OracleChannel:
         self._zsolve_all(dt_eff)
         if cap is not None:
             cap["zsolve"] = (self.u.copy(), self.v.copy(), self.w.copy())
-        self._project(dt_eff, dt_eff, cap)
+        phi = self._project(dt_eff, dt_eff, cap)
+        if self.pressure == "inc":  # solver.py:1001-1012
+            if self.P_curr is None:
+                self.P_curr = phi.copy()
+            elif self.P_prev is None:
+                self.P_prev = self.P_curr.copy()
+                self.P_curr = self.P_curr + phi
+            else:
+                self.P_prev = self.P_curr.copy()
+                self.P_curr = p_ext + phi
+            self.p = self.P_curr
         if cap is not None:
             cap["proj"] = (self.u.copy(), self.v.copy(), self.w.copy())
         self.dt_prev = dt

@@ -1173,6 +1173,10 @@ int slc_adjoint_step(slc_grid *g, int mode, double *const cur[3], double *const 
         g->err = "dt must be positive";
         return SLC_E_INVALID;
     }
+    if (g->P.traj_order != 2) {
+        g->err = "the adjoint supports the trilinear trajectory (traj_interp_order 2)";
+        return SLC_E_INVALID;
+    }
     if (g->P.n_iters < 1 || g->P.n_iters > kMaxIters) {
         g->err = "the adjoint supports 1 to 4 trajectory iterations";
         return SLC_E_INVALID;

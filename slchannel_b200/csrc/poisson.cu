@@ -510,6 +510,30 @@ __global__ void k_bulk_finish_ens(const EnsInst *__restrict__ ins, int mode)
     }
 }
 
+// u, v, w interiors -= c grad(p), p ghost-shaped (projection.py:250-272 on a
+// ghost-filled pressure); the incremental branch's predictor term
+// -dt_eff grad(2 p^n - p^{n-1}) (solver.py:905-941).
+__global__ void k_grad_sub(SlcParams P, const double *__restrict__ p, double *u, double *v, double *w,
+                           const double *__restrict__ dz_c, double c)
+{
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long n = (long long)nx * ny * nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int k = (int)(t % nz);
+    const int j = (int)((t / nz) % ny);
+    const int i = (int)(t / ((long long)nz * ny));
+    const size_t I = i + 1, J = j + 1, K = k + 1;
+    const size_t psx = (size_t)(ny + 2) * (nz + 2), psy = nz + 2;
+    const size_t usx = (size_t)(ny + 2) * (nz + 2), usy = nz + 2;
+    const size_t vsx = (size_t)(ny + 1) * (nz + 2), vsy = nz + 2;
+    const size_t wsx = (size_t)(ny + 2) * (nz + 1), wsy = nz + 1;
+    const double p0 = p[I * psx + J * psy + K];
+    u[I * usx + J * usy + K] -= c * ((p[(I + 1) * psx + J * psy + K] - p0) / P.dx);
+    v[I * vsx + J * vsy + K] -= c * ((p[I * psx + (J + 1) * psy + K] - p0) / P.dy);
+    if (k < nz - 1) w[I * wsx + J * wsy + K] -= c * ((p[I * psx + J * psy + K + 1] - p0) / dz_c[K]);
+}
+
 }  // namespace
 
 cudaError_t launch_apply_bc(const SlcParams &P, double *u, double *v, double *w, double *p,
@@ -637,6 +661,15 @@ cudaError_t launch_bulk_finish_ens(const EnsInst *ins, int ninst, int mode, cuda
 {
     if (ninst <= 0) return cudaSuccess;
     k_bulk_finish_ens<<<ninst, 256, 0, s>>>(ins, mode);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad_sub(const SlcParams &P, const double *p, TriMut f, const double *dz_c, double c,
+                            cudaStream_t s)
+{
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    k_grad_sub<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, p, f.u, f.v, f.w, dz_c, c);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -26,8 +26,46 @@ __device__ __forceinline__ void sample3(const SlcParams &P, const Vel3 &M, doubl
     ws = tri_sample(M.w, t.ib0, t.ib1, t.txb, t.jb0, t.jb1, t.tyb, t.kf, t.wf0, t.wf1);
 }
 
+// The same with tricubic Lagrange sampling (traj_interp_order 4,
+// semilag.py:206-209, 512-528): the order-4 tensor-product stencils of the
+// field gather on the three trajectory components.  Kept out of line so the
+// trilinear path's register allocation does not carry it.
+__device__ __noinline__ void sample3_o4(const SlcParams &P, const Vel3 &M, double x, double y,
+                                        double z, double &us, double &vs, double &ws)
+{
+    const double zc = clampz(P, z);
+    const int c = face_cell(P, zc);
+    Stencil<4, double> st;
+    build_stencil<0, 4, double>(P, M.u.sx, M.u.sy, x, y, zc, c, st);
+    us = gather_sum<4, double, double>(M.u.p, st);
+    build_stencil<1, 4, double>(P, M.v.sx, M.v.sy, x, y, zc, c, st);
+    vs = gather_sum<4, double, double>(M.v.p, st);
+    build_stencil<2, 4, double>(P, M.w.sx, M.w.sy, x, y, zc, c, st);
+    ws = gather_sum<4, double, double>(M.w.p, st);
+}
+
+// Trajectory sampling order as a template argument: 2 or 4 fixed at compile
+// time, 0 read from P.traj_order at run time.
+template <int TO>
+__device__ __forceinline__ bool traj4(const SlcParams &P)
+{
+    return TO == 4 || (TO == 0 && P.traj_order == 4);
+}
+
+// First fixed-point sample at the arrival point (i, j, k) of component C:
+// exact node values for trilinear sampling, the stencils for tricubic.
+template <int C, int TO = 0>
+__device__ __forceinline__ void first_sample(const SlcParams &P, const Vel3 &M, int i, int j, int k,
+                                             double xa, double ya, double za, double &us0,
+                                             double &vs0, double &ws0)
+{
+    if (traj4<TO>(P)) sample3_o4(P, M, xa, ya, za, us0, vs0, ws0);
+    else arrival_sample<C>(P, M, i, j, k, NodeValF64(), us0, vs0, ws0);
+}
+
 // Iterated midpoint rule continued from the first-iteration sample
 // (us0, vs0, ws0) taken at the arrival point; returns the unclamped foot.
+template <int TO = 0>
 __device__ __forceinline__ void trace_foot(const SlcParams &P, const Vel3 &M, double xa, double ya,
                                            double za, double half_dt, double us0, double vs0,
                                            double ws0, double &xd, double &yd, double &zd)
@@ -37,7 +75,8 @@ __device__ __forceinline__ void trace_foot(const SlcParams &P, const Vel3 &M, do
     double zm = clampz(P, za - half_dt * ws0);
     for (int it = 1; it < P.n_iters; ++it) {
         double us, vs, ws;
-        sample3(P, M, xm, ym, zm, us, vs, ws);
+        if (traj4<TO>(P)) sample3_o4(P, M, xm, ym, zm, us, vs, ws);
+        else sample3(P, M, xm, ym, zm, us, vs, ws);
         xm = xa - half_dt * us;
         ym = ya - half_dt * vs;
         zm = clampz(P, za - half_dt * ws);

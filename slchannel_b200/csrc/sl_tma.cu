@@ -164,7 +164,7 @@ __device__ __forceinline__ double gather_global(const SlcParams &P, NodeView<dou
 
 template <int C, int O>
 __global__ void __launch_bounds__(kThreads, 2)
-    k_sl_tma(SlcParams P, Vel3 M, const double *__restrict__ fn, const double *__restrict__ fnm1,
+    k_sl_tma(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, const double *__restrict__ fn, const double *__restrict__ fnm1,
              double dt, double *__restrict__ out, unsigned long long *nclamp, unsigned long long *stats,
              const __grid_constant__ CUtensorMap tmN, const __grid_constant__ CUtensorMap tmM)
 {
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     Foot Fn{}, Fm{};
     if (act) {
         arrival_point<C>(P, i, j, k, xa, ya, za);
-        arrival_sample<C>(P, M, i, j, k, NodeValF64(), us0, vs0, ws0);
+        first_sample<C>(P, M, i, j, k, xa, ya, za, us0, vs0, ws0);
         trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xn, yn, zn);
         trace_foot(P, M, xa, ya, za, dt, us0, vs0, ws0, xm, ym, zm);  // half of 2 dt
         Fn = locate_foot<C, O>(P, xn, yn, zn, i0, j0, ncl);

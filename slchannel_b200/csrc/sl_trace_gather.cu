@@ -31,7 +31,7 @@ constexpr int kTileK = 64, kTileJ = kThreads / kTileK;
 // One arrival point (i, j, k) of component C; out-of-range points only
 // contribute nothing.  Shared by the single-grid kernel below and the
 // persistent ensemble kernel, so both do the same arithmetic per point.
-template <int C, int O, int MODE>
+template <int C, int O, int MODE, int TO = 0>
 __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
                                          const double *__restrict__ fn,
                                          const double *__restrict__ fnm1, double dt,
@@ -43,11 +43,11 @@ __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
         double xa, ya, za;
         arrival_point<C>(P, i, j, k, xa, ya, za);
         double us0, vs0, ws0;
-        arrival_sample<C>(P, M, i, j, k, NodeValF64(), us0, vs0, ws0);
+        first_sample<C, TO>(P, M, i, j, k, xa, ya, za, us0, vs0, ws0);
 
         const NodeView<double> Fn = ghost_view<double>(C, fn, P.nx, P.ny, P.nz);
         double xd, yd, zd;
-        trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd, yd, zd);
+        trace_foot<TO>(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd, yd, zd);
         const double ubar = gather_foot<C, O>(P, Fn, xd, yd, zd, ncl);
         double res;
         if (MODE == 0) {
@@ -56,7 +56,7 @@ __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
             res = ubar + dt * xy_diffusion<C>(P, fn, i, j, k);
         } else {
             const NodeView<double> Fm = ghost_view<double>(C, fnm1, P.nx, P.ny, P.nz);
-            trace_foot(P, M, xa, ya, za, dt, us0, vs0, ws0, xd, yd, zd);  // half of 2 dt
+            trace_foot<TO>(P, M, xa, ya, za, dt, us0, vs0, ws0, xd, yd, zd);  // half of 2 dt
             const double ubb = gather_foot<C, O>(P, Fm, xd, yd, zd, ncl);
             const double Rn = xy_diffusion<C>(P, fn, i, j, k);
             const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion<C>(P, fnm1, i, j, k);
@@ -68,8 +68,8 @@ __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
     }
 }
 
-template <int C, int O, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) k_sl(SlcParams P, Vel3 M, const double *__restrict__ fn,
+template <int C, int O, int MODE, int TO>
+__global__ void __launch_bounds__(kThreads, 2) k_sl(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, const double *__restrict__ fn,
                                                     const double *__restrict__ fnm1, double dt,
                                                     double *__restrict__ out,
                                                     unsigned long long *nclamp)
@@ -78,12 +78,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_sl(SlcParams P, Vel3 M, const d
     const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
     const int i = blockIdx.z;
     unsigned ncl = 0;
-    sl_point<C, O, MODE>(P, M, fn, fnm1, dt, out, i, j, k, ncl);
+    sl_point<C, O, MODE, TO>(P, M, fn, fnm1, dt, out, i, j, k, ncl);
     add_clamps(nclamp, ncl);
 }
 
 template <int C>
-__global__ void __launch_bounds__(kThreads) k_departure(SlcParams P, Vel3 M, double dt,
+__global__ void __launch_bounds__(kThreads) k_departure(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, double dt,
                                                         double *xd, double *yd, double *zd)
 {
     const int nzi = (C == 2) ? P.nz - 1 : P.nz;
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kThreads) k_departure(SlcParams P, Vel3 M, dou
     double xa, ya, za;
     arrival_point<C>(P, i, j, k, xa, ya, za);
     double us0, vs0, ws0;
-    arrival_sample<C>(P, M, i, j, k, NodeValF64(), us0, vs0, ws0);
+    first_sample<C>(P, M, i, j, k, xa, ya, za, us0, vs0, ws0);
     trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd[p], yd[p], zd[p]);
 }
 
@@ -219,16 +219,24 @@ __global__ void k_lincomb_ens(const EnsInst *__restrict__ ins, const EnsItem *__
     }
 }
 
+template <int O, int MODE, int TO>
+void launch_sl_tt(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
+                  unsigned long long *ncl, cudaStream_t s)
+{
+    const dim3 gc((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
+    const dim3 gw((P.nz - 1 + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
+    k_sl<0, O, MODE, TO><<<gc, kThreads, 0, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl);
+    k_sl<1, O, MODE, TO><<<gc, kThreads, 0, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl);
+    if (P.nz > 1) k_sl<2, O, MODE, TO><<<gw, kThreads, 0, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl);
+    count_launches(P.nz > 1 ? 3 : 2);
+}
+
 template <int O, int MODE>
 void launch_sl_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
                  unsigned long long *ncl, cudaStream_t s)
 {
-    const dim3 gc((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
-    const dim3 gw((P.nz - 1 + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
-    k_sl<0, O, MODE><<<gc, kThreads, 0, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl);
-    k_sl<1, O, MODE><<<gc, kThreads, 0, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl);
-    if (P.nz > 1) k_sl<2, O, MODE><<<gw, kThreads, 0, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl);
-    count_launches(P.nz > 1 ? 3 : 2);
+    if (P.traj_order == 4) launch_sl_tt<O, MODE, 4>(P, M, fn, fnm1, dt, out, ncl, s);
+    else launch_sl_tt<O, MODE, 2>(P, M, fn, fnm1, dt, out, ncl, s);
 }
 
 }  // namespace

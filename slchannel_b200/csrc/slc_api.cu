@@ -319,8 +319,10 @@ int slc_grid_create(const slc_grid_desc *d, slc_grid **out)
     *out = nullptr;
     if (d->order != 4 && d->order != 6)
         return fail(nullptr, SLC_E_INVALID, "sl.interp_order must be 4 (tricubic) or 6 (triquintic), got " + std::to_string(d->order));
-    if (d->traj_order != 2)
-        return fail(nullptr, SLC_E_INVALID, "sl.traj_interp_order " + std::to_string(d->traj_order) + " is not implemented (2 = trilinear is)");
+    if (d->traj_order != 2 && d->traj_order != 4)
+        return fail(nullptr, SLC_E_INVALID, "sl.traj_interp_order must be 2 (trilinear) or 4 (tricubic), got " + std::to_string(d->traj_order));
+    if (d->traj_order == 4 && d->precision == SLC_PREC_MIXED)
+        return fail(nullptr, SLC_E_INVALID, "the mixed form samples the trajectory trilinearly (traj_interp_order 2)");
     if (d->n_traj_iters < 1)
         return fail(nullptr, SLC_E_INVALID, "sl.n_traj_iters must be >= 1");
     if (d->stretching != 0 && d->stretching != 1)
@@ -354,6 +356,7 @@ int slc_grid_create(const slc_grid_desc *d, slc_grid **out)
     P.symmetric = d->stretching == 0;
     P.order = d->order;
     P.n_iters = d->n_traj_iters;
+    P.traj_order = d->traj_order;
     P.top_neumann = d->top_wall_neumann ? 1 : 0;
     P.xy_lagged = d->xy_rhs_lagged ? 1 : 0;
     g->mixed = d->precision == SLC_PREC_MIXED ? 1 : 0;
@@ -788,6 +791,44 @@ int slc_gather_stats(slc_grid *g, int64_t *out4, int reset)
     SLC_CK(cudaMemcpy(h, g->dev_flags, sizeof(h), cudaMemcpyDeviceToHost), "read gather stats");
     for (int q = 0; q < 4; ++q) out4[q] = (int64_t)h[q];
     if (reset) SLC_CK(cudaMemset(g->dev_flags, 0, sizeof(h)), "reset gather stats");
+    return SLC_OK;
+}
+
+int slc_step_bdf2_inc(slc_grid *g, double *const cur[3], double *const prev[3], double *const next[3],
+                      double *p_cur, double *p_prev, int have_prev, double dt, int64_t *nclamp,
+                      void *stream)
+{
+    if (!g) return fail(nullptr, SLC_E_INVALID, "null handle");
+    if (!cur || !prev || !next || !p_cur || !p_prev) return fail(g, SLC_E_INVALID, "null pointer");
+    for (int c = 0; c < 3; ++c)
+        if (!cur[c] || !prev[c] || !next[c]) return fail(g, SLC_E_INVALID, "null field pointer");
+    if (!(dt > 0.0)) return fail(g, SLC_E_INVALID, "dt must be positive");
+    DeviceGuard dg(g->device);
+    cudaStream_t s = S(stream);
+    const size_t np = g->ghost_elems[3];
+    if (!g->p_ext) {
+        int rc = dalloc(g, &g->p_ext, np, "extrapolated pressure");
+        if (!rc) rc = dalloc(g, &g->phi, np, "pressure increment");
+        if (rc) return rc;
+    }
+    int rc = do_apply_bc(g, cur[0], cur[1], cur[2], s);
+    if (rc) return rc;
+    rc = do_trace_gather_bdf2(g, cur, prev, dt, next, nclamp, s);
+    if (rc) return rc;
+    const double dt_eff = (2.0 / 3.0) * dt;
+    // p_ext = 2 p^n - p^{n-1}, or p^n on the first BDF2 step after a bootstrap
+    if (have_prev)
+        SLC_CK(launch_lincomb(p_cur, p_prev, 2.0, -1.0, g->p_ext, (int64_t)np, s), "p_ext");
+    else
+        SLC_CK(cudaMemcpyAsync(g->p_ext, p_cur, np * sizeof(double), cudaMemcpyDeviceToDevice, s), "p_ext");
+    SLC_CK(launch_grad_sub(g->P, g->p_ext, TriMut{next[0], next[1], next[2]}, g->dzc, dt_eff, s),
+           "predictor pressure gradient");
+    rc = do_zsolve(g, next[0], next[1], next[2], dt_eff, s);
+    if (!rc) rc = do_project(g, next[0], next[1], next[2], g->phi, dt_eff, dt_eff, s);
+    if (rc) return rc;
+    // p^{n-1} <- p^n, p^{n+1} = p_ext + phi (solver.py:1001-1012)
+    SLC_CK(cudaMemcpyAsync(p_prev, p_cur, np * sizeof(double), cudaMemcpyDeviceToDevice, s), "p history");
+    SLC_CK(launch_lincomb(g->p_ext, g->phi, 1.0, 1.0, p_cur, (int64_t)np, s), "p update");
     return SLC_OK;
 }
 

@@ -14,6 +14,7 @@ struct SlcParams {
     int symmetric;     // tanh map: 1 symmetric, 0 bottom
     int order;         // field interpolation order (4 or 6)
     int n_iters;       // midpoint fixed-point iterations
+    int traj_order;    // trajectory sampling: 2 trilinear, 4 tricubic Lagrange
     int top_neumann;   // free-slip top wall for u, v
     int xy_lagged;     // BDF2 explicit xy-rhs: 0 extrap (2R^n - R^{n-1}), 1 lagged (R^n)
     double dx, dy, inv_dx, inv_dy, inv_dx2, inv_dy2;

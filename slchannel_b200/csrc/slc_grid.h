@@ -35,6 +35,7 @@ struct slc_grid {
     bool mixed_ready = false;
     MixedWS mws{};
     AdjWS *adj = nullptr;
+    double *p_ext = nullptr, *phi = nullptr;  // incremental-pressure workspaces
     HostStep *host = nullptr;
     TmaSL tma{};
     int tma_state = 0;        // 0 not tried, 1 ready, -1 unavailable (L1 gather path)

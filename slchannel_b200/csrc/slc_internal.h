@@ -78,6 +78,10 @@ cudaError_t launch_bulk_finish(const SlcParams &P, const double *partials, doubl
                                double U_bulk, double dt, double *bulk_out, double *shift_out,
                                cudaStream_t s);
 
+// u, v, w interiors -= c grad(p) for a ghost-shaped p (the inc branch).
+cudaError_t launch_grad_sub(const SlcParams &P, const double *p, TriMut f, const double *dz_c, double c,
+                            cudaStream_t s);
+
 constexpr int kBulkBlocks = 1184;  // 8 x 148 SMs; fixed, so the sum order is too
 
 // Message of a failed handle-free call, for slc_last_error(NULL); returns code.

@@ -103,7 +103,7 @@ def _desc(flow, order, keep):
     d.Lx, d.Ly, d.Lz = float(flow.Lx), float(flow.Ly), float(flow.Lz)
     d.gamma = float(flow.gamma)
     d.stretching = 0 if flow.stretching_type == "symmetric" else 1
-    d.order, d.traj_order, d.n_traj_iters = int(order), 2, int(flow.sl_traj_iters)
+    d.order, d.traj_order, d.n_traj_iters = int(order), int(flow.sl_traj_order), int(flow.sl_traj_iters)
     d.top_wall_neumann = 1 if flow.top_wall_bc_type == "neumann" else 0
     d.precision = N.PREC_FP64 if flow.sl_interp_dtype == "fp64" else N.PREC_MIXED
     d.nu = float(flow.nu)

@@ -94,8 +94,6 @@ class SLChannelFlow:
         if self.sl_bdf2_xy_rhs not in ["extrap", "lagged"]:
             raise ValueError(
                 f"sl.bdf2_xy_rhs must be 'extrap' or 'lagged', got {self.sl_bdf2_xy_rhs}")
-        if self.sl_bdf2_pressure == "inc":
-            raise NotImplementedError("sl.bdf2_pressure 'inc' is not implemented on the GPU path")
         solver_type = config.get("solver", {}).get("type", "fft")
         if solver_type != "fft":
             raise ValueError(f"solver.type must be 'fft', got {solver_type!r}.")
@@ -151,6 +149,9 @@ class SLChannelFlow:
         self.u_nm1 = self.v_nm1 = self.w_nm1 = None
         self._next = None
         self._dt_prev_step = None
+        # incremental pressure (sl.bdf2_pressure: inc): p^{n-1} and whether it holds one
+        self._p_prev = None
+        self._p_have_prev = False
         if allocate_fields:
             self._save_and_project_initial()
 
@@ -192,6 +193,7 @@ class SLChannelFlow:
         self.u_nm1 = self.v_nm1 = self.w_nm1 = None
         self._next = None
         self._dt_prev_step = None
+        self._p_have_prev = False
         self._check_state()
 
     def compute_divergence(self):
@@ -232,6 +234,7 @@ class SLChannelFlow:
         self.u, self.v, self.w = nxt
         self._next = old if old[0] is not None else None
         self._dt_prev_step = dt
+        self._p_have_prev = False  # the bootstrap's p is its phi (solver.py:802-807)
         return self._bdf2_forcing_update(dt)
 
     def step_sl_bdf2(self, dt):
@@ -254,8 +257,16 @@ class SLChannelFlow:
         pc, kc = N.ptr_array(cur)
         pp, kp = N.ptr_array(prev)
         pn, kn = N.ptr_array(nxt)
-        self._grid.call("slc_step_bdf2", pc, pp, pn, N.ptr(self.p), dt,
-                        N.ptr(self.sl.n_clamped_last), self._stream())
+        if self.sl_bdf2_pressure == "inc":
+            if self._p_prev is None:
+                self._p_prev = torch.zeros_like(self.p)
+            self._grid.call("slc_step_bdf2_inc", pc, pp, pn, N.ptr(self.p), N.ptr(self._p_prev),
+                            1 if self._p_have_prev else 0, dt, N.ptr(self.sl.n_clamped_last),
+                            self._stream())
+            self._p_have_prev = True
+        else:
+            self._grid.call("slc_step_bdf2", pc, pp, pn, N.ptr(self.p), dt,
+                            N.ptr(self.sl.n_clamped_last), self._stream())
         self.u_nm1, self.v_nm1, self.w_nm1 = cur
         self.u, self.v, self.w = nxt
         self._next = prev

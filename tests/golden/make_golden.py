@@ -195,6 +195,12 @@ def main(ref_root):
         dict(name="o6_sym", order=6, st="symmetric", top="dirichlet", capture=(1, 3)),
         dict(name="o4_sym", order=4, st="symmetric", top="dirichlet", capture=(3,)),
         dict(name="o4_bottom_neumann", order=4, st="bottom", top="neumann", capture=()),
+        # the incremental pressure branch (solver.py:905-941, 1001-1012) and the
+        # order-4 trajectory sampling (semilag.py:206-209, 512-528)
+        dict(name="o6_inc", order=6, st="symmetric", top="dirichlet", capture=(3,), pressure="inc"),
+        dict(name="o6_traj4", order=6, st="symmetric", top="dirichlet", capture=(3,), traj=4),
+        dict(name="o4_inc_traj4_bottom_neumann", order=4, st="bottom", top="neumann", capture=(),
+             pressure="inc", traj=4),
     ]
     snx, sny, snz = 8, 6, 12
     sLx, sLy, sLz = 2 * np.pi, np.pi, 2.0
@@ -216,7 +222,8 @@ def main(ref_root):
                            "n_out": 10**8, "n_save": 10**8},
                 "advection": {"scheme": "sl"},
                 "sl": {"interp_order": case["order"], "n_traj_iters": 2,
-                       "interp_dtype": "fp64"},
+                       "interp_dtype": "fp64", "traj_interp_order": case.get("traj", 2),
+                       "bdf2_pressure": case.get("pressure", "noninc")},
                 "statistics": {"n_stats": 0},
             }
             path = os.path.join(tmp, "cfg.yaml")
@@ -256,6 +263,8 @@ def main(ref_root):
                 "params": np.array([snx, sny, snz, sLx, sLy, sLz, sgamma, Re, dt, case["order"]]),
                 "stretching": np.array(case["st"]),
                 "top": np.array(case["top"]),
+                "pressure": np.array(case.get("pressure", "noninc")),
+                "traj_order": np.array(case.get("traj", 2)),
                 "z_f": szf, "z_c": szc,
                 "init_u": N(s.u), "init_v": N(s.v), "init_w": N(s.w), "init_p": N(s.p),
             }

@@ -52,7 +52,7 @@ def _desc(**over):
 
 @pytest.mark.parametrize(
     "field,value,msg",
-    [("order", 5, "interp_order"), ("traj_order", 4, "traj_interp_order"),
+    [("order", 5, "interp_order"), ("traj_order", 3, "traj_interp_order"),
      ("n_traj_iters", 0, "n_traj_iters"), ("stretching", 3, "stretching"),
      ("precision", 7, "precision"), ("nz", 1, "nz")],
 )

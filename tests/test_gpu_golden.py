@@ -113,11 +113,13 @@ def config_from_step_golden(s):
         "initialization": {"type": "parabolic"},
         "time": {"dt": float(dt)},
         "compute": {"device": "cuda"},
-        "sl": {"interp_order": int(order), "n_traj_iters": 2, "interp_dtype": "fp64"},
+        "sl": {"interp_order": int(order), "n_traj_iters": 2, "interp_dtype": "fp64",
+               "traj_interp_order": int(s["traj_order"]) if "traj_order" in s.files else 2,
+               "bdf2_pressure": str(s["pressure"]) if "pressure" in s.files else "noninc"},
     }, float(dt)
 
 
-CASES = ["o6_sym", "o4_sym", "o4_bottom_neumann"]
+CASES = ["o6_sym", "o4_sym", "o4_bottom_neumann", "o6_inc", "o6_traj4", "o4_inc_traj4_bottom_neumann"]
 
 
 @pytest.mark.parametrize("name", CASES)

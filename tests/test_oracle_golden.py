@@ -93,13 +93,17 @@ def test_advect_golden(adv_golden, order):
 def oracle_from_step_golden(s):
     nx, ny, nz, Lx, Ly, Lz, gamma, Re, dt, order = s["params"]
     nx, ny, nz, order = int(nx), int(ny), int(nz), int(order)
+    pressure = str(s["pressure"]) if "pressure" in s.files else "noninc"
+    traj = int(s["traj_order"]) if "traj_order" in s.files else 2
     ch = OracleChannel(nx, ny, nz, Lx, Ly, Lz, gamma, 1.0 / Re, s["init_u"], s["init_v"],
                        s["init_w"], s["init_p"], stretching_type=str(s["stretching"]),
-                       order=order, top_wall_bc_type=str(s["top"]), z_f=s["z_f"], z_c=s["z_c"])
+                       order=order, top_wall_bc_type=str(s["top"]), z_f=s["z_f"], z_c=s["z_c"],
+                       traj_order=traj, bdf2_pressure=pressure)
     return ch, float(dt)
 
 
-@pytest.mark.parametrize("name", ["o6_sym", "o4_sym", "o4_bottom_neumann"])
+@pytest.mark.parametrize("name", ["o6_sym", "o4_sym", "o4_bottom_neumann", "o6_inc", "o6_traj4",
+                                  "o4_inc_traj4_bottom_neumann"])
 def test_step_golden(name):
     s = load_golden(f"step_{name}.npz")
     ch, dt = oracle_from_step_golden(s)
