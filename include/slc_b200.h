@@ -285,6 +285,34 @@ SLC_API int slc_timing_read(slc_grid *g, double *ms, int64_t *count);
  * far-foot boxes staged (the rest gathered through L1).  Synchronous. */
 SLC_API int slc_gather_stats(slc_grid *g, int64_t *out4, int reset);
 
+/* ---- Diagnostics and statistics (on the device, no host synchronisation) ----
+ * out4 (device, 4 doubles) <- [max |div| over the interior (utils.py:166-180),
+ * u_tau (utils.py:116-144: wall-adjacent plane means of u, ghosts included,
+ * bottom only for a free-slip top), the CFL inverse max(1/dt) of
+ * compute_cfl_fused (operators.py:839-940), the bulk velocity
+ * (utils.py:147-163)].  Fixed-order reductions: reruns agree bit for bit.
+ * The raw form needs no handle; scratch holds
+ * slc_diagnostics_scratch_doubles() device doubles and z_c nz+2 centres. */
+SLC_API int slc_diagnostics(slc_grid *g, const double *u, const double *v, const double *w, double *out4,
+                            void *stream);
+SLC_API int slc_diagnostics_scratch_doubles(void);
+SLC_API int slc_diagnostics_raw(int nx, int ny, int nz, double dx, double dy, const double *dz_f,
+                                const double *dz_c, const double *z_c, double nu, int top_neumann,
+                                double Lx, double Ly, double Lz, const double *u, const double *v,
+                                const double *w, double *out4, double *scratch, void *stream);
+
+/* One snapshot of TurbulenceStats.accumulate_statistics (turbstats.py:156-360)
+ * added to device accumulators:
+ *  - prof (11 nz doubles, or NULL): U, u'u', v'v', w'w', u'w', V, W, U^2, V^2,
+ *    W^2 and U W, each an nz-level profile about the instantaneous plane
+ *    means, as the reference forms them;
+ *  - spec (4 (nx/2) (ny/2) doubles, or NULL): the folded 2-D spectra
+ *    E_uu, E_vv, E_ww, E_uw, averaged over the interior levels k_bot and
+ *    k_top (1-based, as the reference's k_bot / k_top; w negated at the top).
+ * Fixed-order reductions. */
+SLC_API int slc_stats_accumulate(slc_grid *g, const double *u, const double *v, const double *w,
+                                 double *prof, double *spec, int k_bot, int k_top, void *stream);
+
 /* Number of kernels this library has launched in the process so far (its
  * own kernels; cuFFT's are not counted). */
 SLC_API int64_t slc_kernel_launches(void);

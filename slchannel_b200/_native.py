@@ -84,6 +84,10 @@ SIGNATURES = {
     "slc_timing_read": ([_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_L)], _I),
     "slc_kernel_launches": ([], _L),
     "slc_gather_stats": ([_P, ctypes.POINTER(_L), _I], _I),
+    "slc_diagnostics": ([_P, _P, _P, _P, _P, _P], _I),
+    "slc_diagnostics_scratch_doubles": ([], _I),
+    "slc_diagnostics_raw": ([_I, _I, _I, _D, _D, _P, _P, _P, _D, _I, _D, _D, _D, _P, _P, _P, _P, _P, _P], _I),
+    "slc_stats_accumulate": ([_P, _P, _P, _P, _P, _P, _I, _I, _P], _I),
     "slc_zsolve_noalloc": ([_I, _I, _I, _D, _I, _P, _P, _D, _P, _P, _P, _P], _I),
     "slc_adjoint_bc": ([_P, _P, _P, _P, _P], _I),
     "slc_adjoint_step": ([_P, _I, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),

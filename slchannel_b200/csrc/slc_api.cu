@@ -512,6 +512,7 @@ int slc_grid_destroy(slc_grid *g)
     for (cudaEvent_t e : g->evs) cudaEventDestroy(e);
     for (void *p : g->allocs) cudaFree(p);
     if (g->adj) adj_free(g->adj);
+    if (g->stats) stats_free(g->stats);
     if (g->host) {
         cudaDeviceSynchronize();  // copies in flight may still use the host buffers
         host_step_free(g->host);

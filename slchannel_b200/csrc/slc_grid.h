@@ -14,6 +14,8 @@ struct AdjWS;                 // adjoint workspace (adjoint.cu), allocated on fi
 void adj_free(AdjWS *w);
 struct HostStep;              // host-state step machinery (host_step.cu), on first use
 void host_step_free(HostStep *h);
+struct StatsWS;               // diagnostics / statistics workspace (diagnostics.cu), on first use
+void stats_free(StatsWS *s);
 
 struct slc_grid {
     SlcParams P{};
@@ -37,6 +39,7 @@ struct slc_grid {
     AdjWS *adj = nullptr;
     double *p_ext = nullptr, *phi = nullptr;  // incremental-pressure workspaces
     HostStep *host = nullptr;
+    StatsWS *stats = nullptr;
     TmaSL tma{};
     int tma_state = 0;        // 0 not tried, 1 ready, -1 unavailable (L1 gather path)
     unsigned long long *dev_flags = nullptr;  // staged-gather statistics (launch_sl_tma)

@@ -196,6 +196,15 @@ class SLChannelFlow:
         self._p_have_prev = False
         self._check_state()
 
+    def diagnostics(self):
+        """(max |div|, u_tau, CFL inverse, u_bulk) of the current state as a
+        4-element device tensor, from one fused on-device reduction (no host
+        synchronisation; utils.py:116-180, operators.py:839-940)."""
+        out = torch.empty(4, dtype=torch.float64, device=self.device)
+        self._grid.call("slc_diagnostics", N.ptr(self.u), N.ptr(self.v), N.ptr(self.w), N.ptr(out),
+                        self._stream())
+        return out
+
     def compute_divergence(self):
         return compute_divergence(self.u, self.v, self.w, self.nx, self.ny, self.nz, self.dx,
                                   self.dy, self.dz_f)

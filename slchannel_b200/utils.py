@@ -107,3 +107,41 @@ def load_flow_fields(filepath, device="cpu"):
             "Lx": float(data["Lx"]), "Ly": float(data["Ly"]), "step": int(data["step"]),
             "time": float(data["time"]), "u_tau": float(data["u_tau"]),
             "forcing": float(data["forcing"])}
+
+
+def _diag_raw(u, v, w, nx, ny, nz, dx, dy, dz_f, dz_c, z_c, nu, top_wall_bc_type, Lx, Ly, Lz):
+    dev = u.device
+    out = torch.empty(4, dtype=torch.float64, device=dev)
+    scratch = torch.empty(N.lib().slc_diagnostics_scratch_doubles(), dtype=torch.float64, device=dev)
+    f = lambda t: t.to(device=dev, dtype=torch.float64).contiguous()  # noqa: E731
+    dzf, dzc, zc = f(dz_f), f(dz_c), f(z_c)
+    rc = N.lib().slc_diagnostics_raw(int(nx), int(ny), int(nz), float(dx), float(dy), N.ptr(dzf),
+                                     N.ptr(dzc), N.ptr(zc), float(nu),
+                                     1 if top_wall_bc_type == "neumann" else 0, float(Lx), float(Ly),
+                                     float(Lz), N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(out),
+                                     N.ptr(scratch), N.stream_of(u))
+    N.check(rc, None)
+    return out
+
+
+def compute_u_tau(u, z_c, nu, top_wall_bc_type="dirichlet"):
+    """utils.py:116-144 -- friction velocity from the wall-adjacent plane
+    means of u (one-sided difference to the wall), on the device; a 0-D
+    tensor.  Bottom wall only for a free-slip top."""
+    N.require(u, tuple(u.shape), "u")
+    nx, ny, nz = u.shape[0] - 1, u.shape[1] - 2, u.shape[2] - 2
+    v = torch.zeros(nx + 2, ny + 1, nz + 2, dtype=torch.float64, device=u.device)
+    w = torch.zeros(nx + 2, ny + 2, nz + 1, dtype=torch.float64, device=u.device)
+    ones = torch.ones(nz + 1, dtype=torch.float64, device=u.device)
+    return _diag_raw(u, v, w, nx, ny, nz, 1.0, 1.0, ones[:nz], ones, z_c, nu, top_wall_bc_type,
+                     1.0, 1.0, 1.0)[1]
+
+
+def compute_cfl_fused(u, v, w, nx, ny, nz, dx, dy, dz_f, dz_c):
+    """operators.py:839-940 -- max over cells and directions of the CFL
+    inverse (|u|/dx + |v|/dy + |w|/dz with the staggered averages), one fused
+    reduction on the device; returns a float (one synchronisation, as the
+    reference's .item())."""
+    zc = torch.ones(nz + 2, dtype=torch.float64, device=u.device)
+    return float(_diag_raw(u, v, w, nx, ny, nz, dx, dy, dz_f, dz_c, zc, 1.0, "dirichlet",
+                           1.0, 1.0, 1.0)[2])
