@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-channel ensemble form")
     ap.add_argument("--ensemble-n", type=int, default=48)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout check")
+    ap.add_argument("--no-schemes", action="store_true",
+                    help="skip the SL vs Eulerian per-time-unit comparison")
     ap.add_argument("--adjoint-fd-dirs", type=int, default=16)
     ap.add_argument("--mixed-report", action="store_true",
                     help="instead of the bench line: the mixed form against the FP64 form over "
@@ -629,6 +631,59 @@ def run_mixed_report(args):
     return 0
 
 
+def measure_schemes():
+    """The reference's scheme comparison (benchmarks/bench_step.py, case
+    re180): 256^3, 4pi x 2pi x 2, Re_b 2792.8, gamma 1.6, vortex initial
+    field; the Eulerian IMEX step at its advective-CFL dt 0.0057 against the
+    SL-BDF2 step at dt 0.0215 (tricubic and triquintic, the mixed form as the
+    reference's fp32_accum64 runs it, and the FP64 form); wall-clock per
+    simulated time unit.  3 warm-up and 10 timed steps each, CUDA events."""
+    import torch
+
+    from slchannel_b200.solver import SLChannelFlow
+
+    dt_e, dt_sl = 0.0057, 0.0215
+
+    def cfg(scheme, order, prec):
+        return {"grid": {"nx": 256, "ny": 256, "nz": 256},
+                "domain": {"Lx": LX, "Ly": LY, "Lz": LZ},
+                "flow": {"Re": RE_B, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": 1.6},
+                "advection": {"scheme": scheme},
+                "sl": {"interp_order": order, "traj_interp_order": 2, "n_traj_iters": 2,
+                       "interp_dtype": prec},
+                "initialization": {"type": "vortices", "perturbation_intensity": 0.05, "n_vortices": 4},
+                "time": {"dt": dt_e}, "compute": {"device": "cuda"}}
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(10):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 10
+
+    ms = {}
+    flow = SLChannelFlow(config=cfg("eulerian", 4, "fp64"))
+    ms["step_eulerian"] = timed(lambda: flow.step_imex(dt_e))
+    del flow
+    for order, name in ((4, "cubic"), (6, "quintic")):
+        for prec in ("fp32_accum64", "fp64"):
+            flow = SLChannelFlow(config=cfg("sl", order, prec))
+            ms[f"step_sl_{name}_{'mixed' if prec != 'fp64' else 'fp64'}"] = timed(lambda f=flow: f.step_sl_bdf2(dt_sl))
+            del flow
+            torch.cuda.empty_cache()
+    cost_e = ms["step_eulerian"] / dt_e / 1000.0
+    per_unit = {k: v / (dt_sl if k.startswith("step_sl") else dt_e) / 1000.0 for k, v in ms.items()}
+    return {"case": "re180 (benchmarks/bench_step.py): 256^3, 4pi x 2pi x 2, Re_b 2792.8, gamma 1.6",
+            "dt_eulerian": dt_e, "dt_sl": dt_sl, "step_ms": ms, "seconds_per_time_unit": per_unit,
+            "sl_speedup_per_time_unit": {k.replace("step_sl_", ""): cost_e / per_unit[k]
+                                         for k in ms if k.startswith("step_sl")}}
+
+
 def run_b200(args):
     import torch
 
@@ -782,6 +837,8 @@ def run_b200(args):
         line["ensemble_mixed"] = measure_ensemble(args.ensemble_n, K, "mixed")
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = measure_adjoint(args.adjoint_fd_dirs)
+    if world == 1 and not args.no_schemes:
+        line["scheme_comparison"] = measure_schemes()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_cpu, desc, threads = cpu_step_sample(n, order, args.cpu_budget_s)
         line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": UNIT, "cores": threads, "kind": "port",

@@ -258,6 +258,24 @@ SLC_API int slc_step_bdf2(slc_grid *g, double *const cur[3], double *const prev[
 #define SLC_PHASE_BULK 5    /* bulk-flux shift */
 #define SLC_NPHASE 6
 
+/* ---- The Eulerian IMEX scheme (the SL step's comparison baseline) ---------
+ * Explicit x,y diffusion minus flux-form advection of u, v, w on the
+ * interiors (compute_momentum_rhs_fused_imex, operators.py:638-832), one
+ * fused pass; ghosts of ru, rv, rw are not written. */
+SLC_API int slc_imex_rhs(slc_grid *g, const double *u, const double *v, const double *w, double *ru,
+                         double *rv, double *rw, void *stream);
+
+/* One IMEX step up to (not including) the bulk shift (step_imex,
+ * solver.py:1055-1135): rhs_cur <- the explicit right-hand side of vel;
+ * vel += dt (1.5 rhs_cur - 0.5 rhs_prev) (forward Euler without a history);
+ * theta-method z-diffusion (theta 0.5: Crank-Nicolson, its explicit half with
+ * the reference's wall closures); projection at dt; p <- phi.  rhs_prev is
+ * used as workspace afterwards: the caller then swaps the two, as the
+ * reference does (solver.py:1081-1083). */
+SLC_API int slc_step_imex(slc_grid *g, double *const vel[3], double *p, double *const rhs_cur[3],
+                          double *const rhs_prev[3], int have_prev, double dt, double theta,
+                          void *stream);
+
 /* Turn per-phase event timing on (1) or off (0) for a handle; resets the
  * accumulated record.  Adds two cudaEventRecord calls per phase per call. */
 SLC_API int slc_timing(slc_grid *g, int enable);

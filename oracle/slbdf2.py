@@ -447,21 +447,127 @@ def zsolve_coefficients(comp, dt, nz, dz_c, dz_f, nu, theta=1.0, top_wall_bc_typ
     return a, b, c
 
 
+def cn_explicit(comp, f, dt, nx, ny, nz, dz_c, dz_f, nu, theta, top_wall_bc_type="dirichlet"):
+    """operators.py:443-461, 610-622 -- (1 - theta) dt nu d2f/dz2 on the
+    interior unknowns, with the reference's wall closures (for w, its stencil
+    on faces m - 1, m, m + 1 for unknown m)."""
+    beta = (1.0 - theta) * dt * nu
+    if comp in ("u", "v"):
+        dl, dr, dc = dz_c[0:nz], dz_c[1 : nz + 1], dz_f[0:nz]
+        F = f[1 : nx + 1, 1 : ny + 1, :]
+        d2 = ((F[:, :, 2 : nz + 2] - F[:, :, 1 : nz + 1]) / dr - (F[:, :, 1 : nz + 1] - F[:, :, 0:nz]) / dl) / dc
+        d2[:, :, 0] = ((F[:, :, 2] - F[:, :, 1]) / dr[0] - 2.0 * F[:, :, 1] / dl[0]) / dc[0]
+        if top_wall_bc_type == "neumann":
+            d2[:, :, nz - 1] = (-(F[:, :, nz] - F[:, :, nz - 1]) / dl[nz - 1]) / dc[nz - 1]
+        else:
+            d2[:, :, nz - 1] = (-2.0 * F[:, :, nz] / dr[nz - 1]
+                                - (F[:, :, nz] - F[:, :, nz - 1]) / dl[nz - 1]) / dc[nz - 1]
+    else:
+        ni = nz - 1
+        dl, dr, dcv = dz_f[0:ni], dz_f[1:nz], dz_c[1:nz]
+        W = f[1 : nx + 1, 1 : ny + 1, :]
+        d2 = np.empty((nx, ny, ni))
+        d2[:, :, 1 : ni - 1] = ((W[:, :, 2:ni] - W[:, :, 1 : ni - 1]) / dr[1 : ni - 1]
+                                - (W[:, :, 1 : ni - 1] - W[:, :, 0 : ni - 2]) / dl[1 : ni - 1]) / dcv[1 : ni - 1]
+        d2[:, :, 0] = ((W[:, :, 1] - W[:, :, 0]) / dr[0] - W[:, :, 0] / dl[0]) / dcv[0]
+        d2[:, :, ni - 1] = (-W[:, :, ni - 1] / dr[ni - 1]
+                            - (W[:, :, ni - 1] - W[:, :, ni - 2]) / dl[ni - 1]) / dcv[ni - 1]
+    return beta * d2
+
+
 def solve_implicit_diffusion(comp, f, dt, nx, ny, nz, dz_c, dz_f, nu, theta=1.0,
                              top_wall_bc_type="dirichlet"):
-    """operators.py:382-630 (theta = 1, the form the SL step uses): returns a
-    new array whose interior solves (I - theta dt nu Dzz) f_new = f."""
-    if theta != 1.0:
-        raise NotImplementedError("the SL-BDF2 step only uses theta = 1")
+    """operators.py:382-630: returns a new array whose interior solves
+    (I - theta dt nu Dzz) f_new = f + (1 - theta) dt nu Dzz f."""
     a, b, c = zsolve_coefficients(comp, dt, nz, dz_c, dz_f, nu, theta, top_wall_bc_type)
     out = f.copy()
     if comp in ("u", "v"):
-        d = f[1 : nx + 1, 1 : ny + 1, 1 : nz + 1].reshape(nx * ny, nz)
-        out[1 : nx + 1, 1 : ny + 1, 1 : nz + 1] = pcr_solve(a, b, c, d).reshape(nx, ny, nz)
+        d = f[1 : nx + 1, 1 : ny + 1, 1 : nz + 1].copy()
+        if theta < 1.0:
+            d += cn_explicit(comp, f, dt, nx, ny, nz, dz_c, dz_f, nu, theta, top_wall_bc_type)
+        out[1 : nx + 1, 1 : ny + 1, 1 : nz + 1] = pcr_solve(a, b, c, d.reshape(nx * ny, nz)).reshape(nx, ny, nz)
     else:
-        d = f[1 : nx + 1, 1 : ny + 1, 1:nz].reshape(nx * ny, nz - 1)
-        out[1 : nx + 1, 1 : ny + 1, 1:nz] = pcr_solve(a, b, c, d).reshape(nx, ny, nz - 1)
+        d = f[1 : nx + 1, 1 : ny + 1, 1:nz].copy()
+        if theta < 1.0:
+            d += cn_explicit(comp, f, dt, nx, ny, nz, dz_c, dz_f, nu, theta)
+        out[1 : nx + 1, 1 : ny + 1, 1:nz] = pcr_solve(a, b, c, d.reshape(nx * ny, nz - 1)).reshape(nx, ny, nz - 1)
     return out
+
+
+def momentum_rhs_imex(u, v, w, nx, ny, nz, dx, dy, dz_c, dz_f, nu):
+    """operators.py:638-832 -- explicit x,y diffusion minus flux-form
+    advection of u, v, w on the interiors (ghosts zero)."""
+    ru, rv, rw = np.zeros_like(u), np.zeros_like(v), np.zeros_like(w)
+    dxi, dyi = 1.0 / dx, 1.0 / dy
+    nudx2, nudy2 = nu * (1.0 / (dx * dx)), nu * (1.0 / (dy * dy))
+    dzfi = (1.0 / dz_f)[None, None, :]
+    X = slice(1, nx + 1)
+    Y = slice(1, ny + 1)
+    Z = slice(1, nz + 1)
+    ue = np.concatenate([u, u[1:2]], axis=0)
+    ui = 0.5 * (ue[1 : nx + 1, Y, Z] + ue[2 : nx + 2, Y, Z])
+    uu_r = ui * ui
+    ui = 0.5 * (ue[0:nx, Y, Z] + ue[1 : nx + 1, Y, Z])
+    duudx = (uu_r - ui * ui) * dxi
+    vi = 0.5 * (v[X, Y, Z] + v[2 : nx + 2, Y, Z])
+    uy = 0.5 * (ue[X, Y, Z] + ue[X, 2 : ny + 2, Z])
+    vu_t = vi * uy
+    vi = 0.5 * (v[X, 0:ny, Z] + v[2 : nx + 2, 0:ny, Z])
+    uy = 0.5 * (ue[X, 0:ny, Z] + ue[X, Y, Z])
+    dvudy = (vu_t - vi * uy) * dyi
+    wi = 0.5 * (w[X, Y, 1 : nz + 1] + w[2 : nx + 2, Y, 1 : nz + 1])
+    uz = 0.5 * (ue[X, Y, Z] + ue[X, Y, 2 : nz + 2])
+    wu_t = wi * uz
+    wi = 0.5 * (w[X, Y, 0:nz] + w[2 : nx + 2, Y, 0:nz])
+    uz = 0.5 * (ue[X, Y, 0:nz] + ue[X, Y, Z])
+    dwudz = (wu_t - wi * uz) * dzfi
+    adv = duudx + dvudy + dwudz
+    d2x = (ue[2 : nx + 2, Y, Z] - 2.0 * ue[X, Y, Z] + ue[0:nx, Y, Z]) * nudx2
+    d2y = (u[X, 2 : ny + 2, Z] - 2.0 * u[X, Y, Z] + u[X, 0:ny, Z]) * nudy2
+    ru[X, Y, Z] = (d2x + d2y) - adv
+    ve = np.concatenate([v, v[:, 1:2]], axis=1)
+    ui = 0.5 * (u[X, Y, Z] + u[X, 2 : ny + 2, Z])
+    vx = 0.5 * (ve[X, Y, Z] + ve[2 : nx + 2, Y, Z])
+    uv_r = ui * vx
+    ui = 0.5 * (u[0:nx, Y, Z] + u[0:nx, 2 : ny + 2, Z])
+    vx = 0.5 * (ve[0:nx, Y, Z] + ve[X, Y, Z])
+    duvdx = (uv_r - ui * vx) * dxi
+    vi = 0.5 * (ve[X, Y, Z] + ve[X, 2 : ny + 2, Z])
+    vv_t = vi * vi
+    vi = 0.5 * (ve[X, 0:ny, Z] + ve[X, Y, Z])
+    dvvdy = (vv_t - vi * vi) * dyi
+    wi = 0.5 * (w[X, Y, 1 : nz + 1] + w[X, 2 : ny + 2, 1 : nz + 1])
+    vz = 0.5 * (ve[X, Y, Z] + ve[X, Y, 2 : nz + 2])
+    wv_t = wi * vz
+    wi = 0.5 * (w[X, Y, 0:nz] + w[X, 2 : ny + 2, 0:nz])
+    vz = 0.5 * (ve[X, Y, 0:nz] + ve[X, Y, Z])
+    dwvdz = (wv_t - wi * vz) * dzfi
+    adv = duvdx + dvvdy + dwvdz
+    d2x = (v[2 : nx + 2, Y, Z] - 2.0 * v[X, Y, Z] + v[0:nx, Y, Z]) * nudx2
+    d2y = (ve[X, 2 : ny + 2, Z] - 2.0 * ve[X, Y, Z] + ve[X, 0:ny, Z]) * nudy2
+    rv[X, Y, Z] = (d2x + d2y) - adv
+    W = slice(1, nz)
+    ui = 0.5 * (u[X, Y, 1:nz] + u[X, Y, 2 : nz + 1])
+    wx = 0.5 * (w[X, Y, W] + w[2 : nx + 2, Y, W])
+    uw_r = ui * wx
+    ui = 0.5 * (u[0:nx, Y, 1:nz] + u[0:nx, Y, 2 : nz + 1])
+    wx = 0.5 * (w[0:nx, Y, W] + w[X, Y, W])
+    duwdx = (uw_r - ui * wx) * dxi
+    vi = 0.5 * (v[X, Y, 1:nz] + v[X, Y, 2 : nz + 1])
+    wy = 0.5 * (w[X, Y, W] + w[X, 2 : ny + 2, W])
+    vw_t = vi * wy
+    vi = 0.5 * (v[X, 0:ny, 1:nz] + v[X, 0:ny, 2 : nz + 1])
+    wy = 0.5 * (w[X, 0:ny, W] + w[X, Y, W])
+    dvwdy = (vw_t - vi * wy) * dyi
+    wi = 0.5 * (w[X, Y, 1:nz] + w[X, Y, 2 : nz + 1])
+    ww_t = wi * wi
+    wi = 0.5 * (w[X, Y, 0 : nz - 1] + w[X, Y, 1:nz])
+    dwwdz = (ww_t - wi * wi) / dz_c[1:nz][None, None, :]
+    adv = duwdx + dvwdy + dwwdz
+    d2x = (w[2 : nx + 2, Y, W] - 2.0 * w[X, Y, W] + w[0:nx, Y, W]) * nudx2
+    d2y = (w[X, 2 : ny + 2, W] - 2.0 * w[X, Y, W] + w[X, 0:ny, W]) * nudy2
+    rw[X, Y, W] = (d2x + d2y) - adv
+    return ru, rv, rw
 
 
 def compute_divergence(u, v, w, nx, ny, nz, dx, dy, dz_f):
@@ -684,6 +790,34 @@ class OracleChannel:
         self.dt_prev = dt
         ub, f = self._bulk_shift(dt)
         return (ub, f, cap) if capture else (ub, f)
+
+    def step_imex(self, dt, theta=0.5):
+        """solver.py:1055-1135 -- AB2 explicit advection + x,y diffusion,
+        Crank-Nicolson z-diffusion, projection at dt, exact bulk shift."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        self.apply_bc()
+        rhs = momentum_rhs_imex(self.u, self.v, self.w, nx, ny, nz, self.dx, self.dy, self.dz_c,
+                                self.dz_f, self.nu)
+        prev = getattr(self, "rhs_prev", None)
+        if prev is None:
+            self.u += dt * rhs[0]
+            self.v += dt * rhs[1]
+            self.w += dt * rhs[2]
+        else:
+            self.u += dt * (1.5 * rhs[0] - 0.5 * prev[0])
+            self.v += dt * (1.5 * rhs[1] - 0.5 * prev[1])
+            self.w += dt * (1.5 * rhs[2] - 0.5 * prev[2])
+        self.rhs_prev = rhs
+        self.apply_bc()
+        self.u = solve_implicit_diffusion("u", self.u, dt, nx, ny, nz, self.dz_c, self.dz_f, self.nu,
+                                          theta, self.top)
+        self.v = solve_implicit_diffusion("v", self.v, dt, nx, ny, nz, self.dz_c, self.dz_f, self.nu,
+                                          theta, self.top)
+        self.w = solve_implicit_diffusion("w", self.w, dt, nx, ny, nz, self.dz_c, self.dz_f, self.nu,
+                                          theta)
+        self.apply_bc()
+        self._project(dt, dt, None)
+        return self._bulk_shift(dt)
 
     def step_bdf2(self, dt, capture=False):
         """solver.py:813-1018 (noninc or inc pressure)."""

@@ -80,6 +80,8 @@ SIGNATURES = {
                        _P, _P], _I),
     "slc_step_bdf2_inc": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), _P, _P, _I,
                            _D, _P, _P], _I),
+    "slc_imex_rhs": ([_P, _P, _P, _P, _P, _P, _P, _P], _I),
+    "slc_step_imex": ([_P, ctypes.POINTER(_P), _P, ctypes.POINTER(_P), ctypes.POINTER(_P), _I, _D, _D, _P], _I),
     "slc_timing": ([_P, _I], _I),
     "slc_timing_read": ([_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_L)], _I),
     "slc_kernel_launches": ([], _L),

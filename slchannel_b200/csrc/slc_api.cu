@@ -299,6 +299,21 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
 
 }  // namespace
 
+// Step pieces for the other translation units (eulerian.cu).
+int slc_internal_zsolve_theta(slc_grid *g, double *u, double *v, double *w, double dt_implicit, cudaStream_t s)
+{
+    return do_zsolve(g, u, v, w, dt_implicit, s);
+}
+int slc_internal_project(slc_grid *g, double *u, double *v, double *w, double *p, double dt_div,
+                         double dt_proj, cudaStream_t s)
+{
+    return do_project(g, u, v, w, p, dt_div, dt_proj, s);
+}
+int slc_internal_apply_bc(slc_grid *g, double *u, double *v, double *w, cudaStream_t s)
+{
+    return do_apply_bc(g, u, v, w, s);
+}
+
 // Record the message of a failed handle-free call (read with slc_last_error(NULL)).
 int slc_report_error(int code, const char *msg)
 {

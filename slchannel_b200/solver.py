@@ -71,8 +71,6 @@ class SLChannelFlow:
         if self.advection_scheme not in ["sl", "eulerian"]:
             raise ValueError(
                 f"advection.scheme must be 'sl' or 'eulerian', got {self.advection_scheme}")
-        if self.advection_scheme != "sl":
-            raise NotImplementedError("slchannel_b200 implements the 'sl' scheme only")
         sl_cfg = config.get("sl", {})
         self.sl_order = sl_cfg.get("interp_order", 4)
         if self.sl_order not in (4, 6):
@@ -149,6 +147,9 @@ class SLChannelFlow:
         self.u_nm1 = self.v_nm1 = self.w_nm1 = None
         self._next = None
         self._dt_prev_step = None
+        # Eulerian IMEX: the explicit right-hand sides of the last two steps
+        self._rhs_cur = self._rhs_prev = None
+        self._rhs_have_prev = False
         # incremental pressure (sl.bdf2_pressure: inc): p^{n-1} and whether it holds one
         self._p_prev = None
         self._p_have_prev = False
@@ -282,13 +283,31 @@ class SLChannelFlow:
         self._dt_prev_step = dt
         return self._bdf2_forcing_update(dt)
 
+    def step_imex(self, dt):
+        """solver.py:1055-1135 -- the Eulerian IMEX step: AB2 explicit
+        advection + x,y diffusion, Crank-Nicolson z-diffusion, projection,
+        exact bulk shift.  Returns (u_bulk, forcing)."""
+        self._check_state()
+        if self._rhs_cur is None:
+            self._rhs_cur = tuple(torch.zeros_like(t) for t in (self.u, self.v, self.w))
+            self._rhs_prev = tuple(torch.zeros_like(t) for t in (self.u, self.v, self.w))
+        pv, k1 = N.ptr_array((self.u, self.v, self.w))
+        pc, k2 = N.ptr_array(self._rhs_cur)
+        pp, k3 = N.ptr_array(self._rhs_prev)
+        self._grid.call("slc_step_imex", pv, N.ptr(self.p), pc, pp,
+                        1 if self._rhs_have_prev else 0, float(dt), 0.5, self._stream())
+        self._rhs_cur, self._rhs_prev = self._rhs_prev, self._rhs_cur
+        self._rhs_have_prev = True
+        return self._apply_bulk_forcing(dt)
+
     def run_steps(self, n, dt=None):
-        """Advance n SL-BDF2 steps at fixed dt (default: time.dt); returns the
-        last (u_bulk, forcing)."""
+        """Advance n steps of the configured scheme at fixed dt (default:
+        time.dt); returns the last (u_bulk, forcing)."""
         dt = self.dt if dt is None else dt
         res = None
+        step = self.step_imex if self.advection_scheme == "eulerian" else self.step_sl_bdf2
         for _ in range(int(n)):
-            res = self.step_sl_bdf2(dt)
+            res = step(dt)
             self.time += dt
             self.current_step += 1
         return res

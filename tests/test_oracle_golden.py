@@ -131,3 +131,27 @@ def test_step_golden(name):
                                interior(c, s[f"s{step}_zsolve_{c}"], nx, ny, nz)) < 1e-12
                 assert rel_err(interior(c, cap["proj"][i], nx, ny, nz),
                                interior(c, s[f"s{step}_proj_{c}"], nx, ny, nz)) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["sym", "bottom_neumann"])
+def test_imex_golden(name):
+    """The oracle's Eulerian IMEX right-hand side and step against the
+    reference's (tests/golden/make_imex_golden.py)."""
+    from oracle.slbdf2 import momentum_rhs_imex
+
+    s = load_golden(f"imex_{name}.npz")
+    nx, ny, nz, Lx, Ly, Lz, gamma, Re, dt = s["params"]
+    nx, ny, nz = int(nx), int(ny), int(nz)
+    ch = OracleChannel(nx, ny, nz, Lx, Ly, Lz, gamma, 1.0 / Re, s["init_u"], s["init_v"], s["init_w"],
+                       s["init_p"], stretching_type=str(s["stretching"]), top_wall_bc_type=str(s["top"]),
+                       z_f=s["z_f"], z_c=s["z_c"])
+    rhs = momentum_rhs_imex(ch.u, ch.v, ch.w, nx, ny, nz, ch.dx, ch.dy, ch.dz_c, ch.dz_f, ch.nu)
+    for c, r in zip("uvw", rhs):
+        assert rel_err(r, s[f"rhs_{c}"]) < 1e-13, c
+    for step in range(1, 5):
+        ub, forcing = ch.step_imex(float(dt))
+        for c in "uvw":
+            assert rel_err(getattr(ch, c), s[f"s{step}_{c}"]) < 1e-12, (step, c)
+        assert rel_err(ch.p, s[f"s{step}_p"]) < 1e-11
+        assert abs(ub - float(s[f"s{step}_ubulk"])) < 1e-13
+        assert abs(forcing - float(s[f"s{step}_forcing"])) < 1e-10
