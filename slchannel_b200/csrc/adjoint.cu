@@ -90,17 +90,18 @@ __device__ __forceinline__ void ubasis_all(const SlcParams &P, double t, double 
 }
 
 template <int O>
-__device__ __forceinline__ double zbasis(const double *zn, const double *dinv, int k0, double z, int m)
+__device__ __forceinline__ double zbasis(const double *zn, const double *dinv, int rows, int k0,
+                                         double z, int m)
 {
     double pr = 1.0;
 #pragma unroll
     for (int l = 0; l < O; ++l)
         if (l != m) pr *= z - __ldg(zn + k0 + l);
-    return pr * __ldg(dinv + k0 * O + m);
+    return pr * __ldg(dinv + m * rows + k0);
 }
 
 template <int O>
-__device__ __forceinline__ void zbasis_all(const double *zn, const double *dinv, int k0, double z,
+__device__ __forceinline__ void zbasis_all(const double *zn, const double *dinv, int rows, int k0, double z,
                                            double (&w)[O], double (&dw)[O])
 {
     double d[O];
@@ -121,7 +122,7 @@ __device__ __forceinline__ void zbasis_all(const double *zn, const double *dinv,
                 if (l != m && l != q) pq *= d[l];
             s += pq;
         }
-        const double di = __ldg(dinv + k0 * O + m);
+        const double di = __ldg(dinv + m * rows + k0);
         w[m] = pr * di;
         dw[m] = s * di;
     }
@@ -166,7 +167,7 @@ __device__ void grad_interp(const SlcParams &P, NodeView<double> F, double x, do
     ubasis_all<O>(P, b.ty, wy, dwy);
     const double *zn = Comp<C>::centers ? P.zc : P.zf;
     const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
-    zbasis_all<O>(zn, dinv, b.k0, z, wz, dwz);
+    zbasis_all<O>(zn, dinv, denom_rows(Comp<C>::centers, P.nz, O), b.k0, z, wz, dwz);
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (int i = 0; i < O; ++i) {
         const int xo = wrapn(b.bx0 + i, P.nx) * F.sx;
@@ -216,12 +217,12 @@ __device__ __forceinline__ TriPiece tri_piece(const SlcParams &P, int c, const T
     }
     if (c < 2) {
         r.k0 = t.kc; r.wz0 = t.wc0; r.wz1 = t.wc1;
-        r.dwz0 = __ldg(P.dinv_c[2] + 2 * t.kc);
-        r.dwz1 = __ldg(P.dinv_c[2] + 2 * t.kc + 1);
+        r.dwz0 = __ldg(P.dinv_c[2] + t.kc);
+        r.dwz1 = __ldg(P.dinv_c[2] + (P.nz + 1) + t.kc);
     } else {
         r.k0 = t.kf; r.wz0 = t.wf0; r.wz1 = t.wf1;
-        r.dwz0 = __ldg(P.dinv_f[2] + 2 * t.kf);
-        r.dwz1 = __ldg(P.dinv_f[2] + 2 * t.kf + 1);
+        r.dwz0 = __ldg(P.dinv_f[2] + t.kf);
+        r.dwz1 = __ldg(P.dinv_f[2] + P.nz + t.kf);
     }
     return r;
 }
@@ -578,7 +579,7 @@ __global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double4 *
                 for (int p = a; p < b; ++p) {
                     const double4 R = pay[__ldg(order + p)];
                     const double w = ubasis<O>(P, R.x, mx) * ubasis<O>(P, R.y, my) *
-                                     zbasis<O>(zn, dinv, k0, R.z, mz);
+                                     zbasis<O>(zn, dinv, NZ - O + 1, k0, R.z, mz);
                     acc = fma(R.w, w, acc);
                 }
             }

@@ -140,12 +140,12 @@ __device__ __forceinline__ void sample3_32(const SlcParams &P, const Vel3M &M, c
     const int c = face_cell32(P, (float)z);
     const int kc = min(max(c + (z >= __ldg(P.zc + c + 1) ? 1 : 0), 0), P.nz);
     const int kf = min(max(c, 0), P.nz - 1);
-    const float *dc = P.dinv_c32[2] + 2 * kc;
-    const float *df = P.dinv_f32[2] + 2 * kf;
+    const float *dc = P.dinv_c32[2] + kc;  // order-2 tables: nz+1 / nz rows
+    const float *df = P.dinv_f32[2] + kf;
     const float wc0 = (float)(z - __ldg(P.zc + kc + 1)) * __ldg(dc);
-    const float wc1 = (float)(z - __ldg(P.zc + kc)) * __ldg(dc + 1);
+    const float wc1 = (float)(z - __ldg(P.zc + kc)) * __ldg(dc + P.nz + 1);
     const float wf0 = (float)(z - __ldg(P.zf + kf + 1)) * __ldg(df);
-    const float wf1 = (float)(z - __ldg(P.zf + kf)) * __ldg(df + 1);
+    const float wf1 = (float)(z - __ldg(P.zf + kf)) * __ldg(df + P.nz);
     us = tri32(M.u, ia0, ia1, txa, jb0, jb1, tyb, kc, wc0, wc1);
     vs = tri32(M.v, ib0, ib1, txb, ja0, ja1, tya, kc, wc0, wc1);
     ws = tri32(M.w, ib0, ib1, txb, jb0, jb1, tyb, kf, wf0, wf1);
@@ -208,7 +208,7 @@ __device__ __forceinline__ double gather_foot32(const SlcParams &P, MixedView F,
     // interpolant in proportion to the field itself
     {
         const double *zn = Comp<C>::centers ? P.zc : P.zf;
-        const float *di = (Comp<C>::centers ? P.dinv_c32[O] : P.dinv_f32[O]) + k0 * O;
+        const float *di = (Comp<C>::centers ? P.dinv_c32[O] : P.dinv_f32[O]) + k0;
         float d[O], pre[O];
 #pragma unroll
         for (int l = 0; l < O; ++l) d[l] = (float)(z - __ldg(zn + k0 + l));
@@ -218,7 +218,7 @@ __device__ __forceinline__ double gather_foot32(const SlcParams &P, MixedView F,
         float suf = 1.f;
 #pragma unroll
         for (int m = O - 1; m >= 0; --m) {
-            st.wz[m] = pre[m] * suf * __ldg(di + m);
+            st.wz[m] = pre[m] * suf * __ldg(di + m * (NZ - O + 1));
             suf = suf * d[m];
         }
     }
@@ -354,7 +354,7 @@ __device__ __forceinline__ void plane_partial(const SlcParams &P, const double *
     }
 }
 
-__global__ void __launch_bounds__(256) k_plane_partials(SlcParams P, MeanSrcs S, double *partials,
+__global__ void __launch_bounds__(256) k_plane_partials(SlcParams P, const __grid_constant__ MeanSrcs S, double *partials,
                                                         int ldp)
 {
     const int f = blockIdx.y;

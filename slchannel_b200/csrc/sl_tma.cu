@@ -133,7 +133,7 @@ __device__ __forceinline__ double gather_box(const SlcParams &P, const double *b
     uniform_weights<O, double>(P, F.ty, wy);
     const double *zn = Comp<C>::centers ? P.zc : P.zf;
     const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
-    z_weights<O, double>(zn, dinv, F.k0, F.z, wz);
+    z_weights<O, double>(zn, dinv, denom_rows(Comp<C>::centers, P.nz, O), F.k0, F.z, wz);
     const double *b = box + (ox * kBY + oy) * kBZ + oz;
     double acc = 0.0;
 #pragma unroll

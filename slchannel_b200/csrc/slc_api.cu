@@ -77,7 +77,8 @@ int upload(slc_grid *g, T **p, const std::vector<T> &h, const char *what)
     return SLC_OK;
 }
 
-// semilag.py:102-114: 1 / prod_{l != m}(z[b+m] - z[b+l]), products in ascending l.
+// semilag.py:102-114: 1 / prod_{l != m}(z[b+m] - z[b+l]), products in ascending l,
+// stored node-major (entry (b, m) at m * nb + b).
 std::vector<double> denom_table(const std::vector<double> &zn, int order)
 {
     const int nb = (int)zn.size() - order + 1;
@@ -91,7 +92,7 @@ std::vector<double> denom_table(const std::vector<double> &zn, int order)
                 prod = first ? d : prod * d;
                 first = false;
             }
-            t[(size_t)b * order + m] = 1.0 / prod;
+            t[(size_t)m * nb + b] = 1.0 / prod;  // node-major (denom_rows)
         }
     return t;
 }

@@ -170,10 +170,19 @@ __device__ __forceinline__ void uniform_weights(const SlcParams &P, T t, T (&w)[
     }
 }
 
+// Lagrange inverse-denominator tables (semilag.py:102-114) are stored
+// node-major: the factor of stencil node m for the stencil starting at z node
+// b is dinv[m * rows + b], rows = NZ - O + 1 stencil starts, so lanes at
+// consecutive b read consecutive words.
+__host__ __device__ inline int denom_rows(bool centers, int nz, int O)
+{
+    return (centers ? nz + 2 : nz + 1) - O + 1;
+}
+
 // Nonuniform Lagrange weights against the actual z nodes (semilag.py:441-454).
 template <int O, typename T>
-__device__ __forceinline__ void z_weights(const T *__restrict__ zn, const T *__restrict__ dinv, int k0,
-                                          T z, T (&w)[O])
+__device__ __forceinline__ void z_weights(const T *__restrict__ zn, const T *__restrict__ dinv,
+                                          int rows, int k0, T z, T (&w)[O])
 {
     T d[O];
 #pragma unroll
@@ -183,10 +192,10 @@ __device__ __forceinline__ void z_weights(const T *__restrict__ zn, const T *__r
 #pragma unroll
     for (int l = 1; l < O; ++l) pre[l] = pre[l - 1] * d[l - 1];
     T suf = (T)1;
-    const T *di = dinv + k0 * O;
+    const T *di = dinv + k0;
 #pragma unroll
     for (int m = O - 1; m >= 0; --m) {
-        w[m] = pre[m] * suf * __ldg(di + m);
+        w[m] = pre[m] * suf * __ldg(di + m * rows);
         suf = suf * d[m];
     }
 }
@@ -229,11 +238,11 @@ __device__ __forceinline__ void build_stencil(const SlcParams &P, int sx, int sy
     const double *zn = Comp<C>::centers ? P.zc : P.zf;
     const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
     if constexpr (sizeof(T) == 8) {
-        z_weights<O, double>(zn, dinv, k0, z, st.wz);
+        z_weights<O, double>(zn, dinv, NZ - O + 1, k0, z, st.wz);
     } else {
         const float *zn32 = Comp<C>::centers ? P.zc32 : P.zf32;
         const float *dinv32 = Comp<C>::centers ? P.dinv_c32[O] : P.dinv_f32[O];
-        z_weights<O, float>(zn32, dinv32, k0, (float)z, st.wz);
+        z_weights<O, float>(zn32, dinv32, NZ - O + 1, k0, (float)z, st.wz);
     }
 }
 
@@ -319,12 +328,12 @@ __device__ __forceinline__ void tri_shared(const SlcParams &P, double x, double 
     const int kf = min(max(c_face, 0), P.nz - 1);
     t.kc = kc;
     t.kf = kf;
-    const double *dc = P.dinv_c[2] + 2 * kc;
-    const double *df = P.dinv_f[2] + 2 * kf;
+    const double *dc = P.dinv_c[2] + kc;  // order-2 tables: nz+1 / nz rows
+    const double *df = P.dinv_f[2] + kf;
     t.wc0 = (z - __ldg(P.zc + kc + 1)) * __ldg(dc);
-    t.wc1 = (z - __ldg(P.zc + kc)) * __ldg(dc + 1);
+    t.wc1 = (z - __ldg(P.zc + kc)) * __ldg(dc + P.nz + 1);
     t.wf0 = (z - __ldg(P.zf + kf + 1)) * __ldg(df);
-    t.wf1 = (z - __ldg(P.zf + kf)) * __ldg(df + 1);
+    t.wf1 = (z - __ldg(P.zf + kf)) * __ldg(df + P.nz);
 }
 
 // Node value accessor for the arrival-point sample below (FP64 node views).
@@ -354,9 +363,9 @@ __device__ __forceinline__ void arrival_sample(const SlcParams &P, const V3 &M, 
         vs = 0.25 * ((val(M.v, i, j, k + 1) + val(M.v, ip, j, k + 1)) +
                      (val(M.v, i, jp, k + 1) + val(M.v, ip, jp, k + 1)));
         const double z = __ldg(P.zc + k + 1);
-        const double *df = P.dinv_f[2] + 2 * k;  // face interval k
+        const double *df = P.dinv_f[2] + k;  // face interval k
         const double w0 = (z - __ldg(P.zf + k + 1)) * __ldg(df);
-        const double w1 = (z - __ldg(P.zf + k)) * __ldg(df + 1);
+        const double w1 = (z - __ldg(P.zf + k)) * __ldg(df + P.nz);
         ws = 0.5 * ((w0 * val(M.w, i, j, k) + w1 * val(M.w, i, j, k + 1)) +
                     (w0 * val(M.w, ip, j, k) + w1 * val(M.w, ip, j, k + 1)));
     } else if (C == 1) {
@@ -364,16 +373,16 @@ __device__ __forceinline__ void arrival_sample(const SlcParams &P, const V3 &M, 
                      (val(M.u, i, jp, k + 1) + val(M.u, ip, jp, k + 1)));
         vs = val(M.v, i, jp, k + 1);
         const double z = __ldg(P.zc + k + 1);
-        const double *df = P.dinv_f[2] + 2 * k;
+        const double *df = P.dinv_f[2] + k;
         const double w0 = (z - __ldg(P.zf + k + 1)) * __ldg(df);
-        const double w1 = (z - __ldg(P.zf + k)) * __ldg(df + 1);
+        const double w1 = (z - __ldg(P.zf + k)) * __ldg(df + P.nz);
         ws = 0.5 * ((w0 * val(M.w, i, j, k) + w1 * val(M.w, i, j, k + 1)) +
                     (w0 * val(M.w, i, jp, k) + w1 * val(M.w, i, jp, k + 1)));
     } else {
         const double z = __ldg(P.zf + k + 1);
-        const double *dc = P.dinv_c[2] + 2 * (k + 1);  // centre interval k+1
+        const double *dc = P.dinv_c[2] + (k + 1);  // centre interval k+1
         const double c0 = (z - __ldg(P.zc + k + 2)) * __ldg(dc);
-        const double c1 = (z - __ldg(P.zc + k + 1)) * __ldg(dc + 1);
+        const double c1 = (z - __ldg(P.zc + k + 1)) * __ldg(dc + P.nz + 1);
         us = 0.5 * ((c0 * val(M.u, i, j, k + 1) + c1 * val(M.u, i, j, k + 2)) +
                     (c0 * val(M.u, ip, j, k + 1) + c1 * val(M.u, ip, j, k + 2)));
         vs = 0.5 * ((c0 * val(M.v, i, j, k + 1) + c1 * val(M.v, i, j, k + 2)) +
