@@ -440,8 +440,17 @@ def measure_mixed(flow64, n, order, K, W, dist):
                    / sum((getattr(flow64, c) ** 2).sum().item() for c in "uvw"))
     div = compute_divergence(flow32.u, flow32.v, flow32.w, n, n, n, flow32.dx, flow32.dy, flow32.dz_f)
     sl_ms, sl_cnt = phases["sl"]
+    from slchannel_b200 import _native as N
+
+    _, flops_alg, pts = sl_algorithmic(n, order)
+    t_sl = sl_ms / 1000.0 / max(sl_cnt, 1)
+    fp32_peak = N.fma_peak_gflops(False)
     return {"value": world * K / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / K,
             "sl_kernel_ms_per_step": sl_ms / max(sl_cnt, 1),
+            "fp32_pipe": {"achieved": flops_alg / t_sl / 1e9, "peak": fp32_peak, "unit": "GFLOP/s",
+                          "frac": flops_alg / t_sl / 1e9 / fp32_peak,
+                          "peak_source": "measured on this GPU: slc_fma_peak (FP32 FMA chains, "
+                                         "best of 3); the gather's arithmetic is mostly FP32"},
             "phase_ms": {p: v[0] / max(v[1], 1) for p, v in phases.items() if v[1]},
             "vs_fp64_after_steps": S, "rel_linf_err_vs_fp64": max(errs), "rel_l2_err_vs_fp64": l2,
             "max_div": float(div.abs().max()),
@@ -749,6 +758,18 @@ def run_b200(args):
         "kernel_ms_per_step": t_sl * 1000.0,
         "fp64_gflops": flops_alg / t_sl / 1e9,
         "note": "the FP64 gather is bound by L1/LSU load throughput and the FP64 pipe, not HBM",
+    }
+    # the same kernel's algorithmic FLOP rate against this GPU's FP64 FMA pipe,
+    # measured here by the library's FMA-chain kernel (MEASURED_PEAKS.json has
+    # no FP64 figure)
+    from slchannel_b200 import _native as N
+
+    fp64_peak = N.fma_peak_gflops(True)
+    roofline["fp64_pipe"] = {
+        "achieved": flops_alg / t_sl / 1e9, "peak": fp64_peak, "unit": "GFLOP/s",
+        "frac": flops_alg / t_sl / 1e9 / fp64_peak,
+        "flops_per_arrival_point": flops_alg / pts,
+        "peak_source": "measured on this GPU: slc_fma_peak (FP64 FMA chains on every SM, best of 3)",
     }
     phase_ms = {p: (v[0] / max(v[1], 1)) for p, v in phases.items() if v[1]}
 

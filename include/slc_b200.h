@@ -335,6 +335,13 @@ SLC_API int slc_stats_accumulate(slc_grid *g, const double *u, const double *v, 
  * own kernels; cuFFT's are not counted). */
 SLC_API int64_t slc_kernel_launches(void);
 
+/* FMA-pipe throughput of the current device in GFLOP/s (FMA = 2 flops),
+ * FP64 (fp64 = 1) or FP32 (fp64 = 0): a register-resident chain kernel over
+ * every SM at full occupancy, best of three timed launches on `stream`
+ * (synchronises it).  Measurement support, no counterpart in the reference:
+ * the denominator for the trace+gather kernels' arithmetic rate. */
+SLC_API int slc_fma_peak(int fp64, double *gflops, void *stream);
+
 /* ---- Adjoint (reverse mode) of the step ----------------------------------------
  * No counterpart in the reference, which relies on torch autograd through its
  * eager path.  Gradients of a loss on the velocity with respect to earlier

@@ -91,6 +91,7 @@ SIGNATURES = {
     "slc_diagnostics_raw": ([_I, _I, _I, _D, _D, _P, _P, _P, _D, _I, _D, _D, _D, _P, _P, _P, _P, _P, _P], _I),
     "slc_stats_accumulate": ([_P, _P, _P, _P, _P, _P, _I, _I, _P], _I),
     "slc_zsolve_noalloc": ([_I, _I, _I, _D, _I, _P, _P, _D, _P, _P, _P, _P], _I),
+    "slc_fma_peak": ([_I, _P, _P], _I),
     "slc_adjoint_bc": ([_P, _P, _P, _P, _P], _I),
     "slc_adjoint_step": ([_P, _I, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
                           ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P], _I),
@@ -235,6 +236,15 @@ class Grid:
 
 def kernel_launches():
     return int(lib().slc_kernel_launches())
+
+
+def fma_peak_gflops(fp64=True, stream=None):
+    """Measured FMA-pipe throughput (GFLOP/s) of the current device, FP64 or
+    FP32, from the library's register-resident FMA-chain kernel."""
+    out = ctypes.c_double(0.0)
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(lib().slc_fma_peak(1 if fp64 else 0, ctypes.byref(out), ctypes.c_void_p(s)), None)
+    return out.value
 
 
 def ptr_array(tensors):

@@ -141,15 +141,19 @@ __device__ __forceinline__ void div_pack_tile(const SlcParams &P, const double *
 {
     __shared__ double tile[32][33];
     const int i = bz, j0 = by * 32, k0 = bx * 32;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    for (int r = ty; r < 32; r += 8) {
-        const int j = j0 + r, k = k0 + tx;
-        double val = 0.0;
-        if (j < P.ny && k < P.nz) val = div_at(P, u, v, w, dz_f, i, j, k) / dt_div;
-        tile[r][tx] = val;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // block (32, 8): rows ty + 8q
+    double val[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {  // all four rows' loads in flight together
+        const int j = j0 + ty + 8 * q, k = k0 + tx;
+        val[q] = (j < P.ny && k < P.nz) ? div_at(P, u, v, w, dz_f, i, j, k) / dt_div : 0.0;
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) tile[ty + 8 * q][tx] = val[q];
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int r = ty + 8 * q;
         const int k = k0 + r, j = j0 + tx;
         if (k < P.nz && j < P.ny) rhs[((size_t)k * P.nx + i) * P.ny + j] = tile[tx][r];
     }
@@ -299,16 +303,31 @@ __device__ __forceinline__ void project_tile(const SlcParams &P, const double *_
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int i = bz, j0 = by * 32, k0 = bx * 32;
     const int i1 = (i + 1 == nx) ? 0 : i + 1;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    for (int r = ty; r < 33; r += 8) {
-        const int k = k0 + r;
-        if (k >= nz) continue;
-        for (int c = tx; c < 33; c += 32) {
-            int j = j0 + c;
-            if (j > ny) continue;
-            if (j == ny) j = 0;
-            t0[r][c] = phi[((size_t)k * nx + i) * ny + j];
-            if (r < 32 && c < 32) t1[r][c] = phi[((size_t)k * nx + i1) * ny + j];
+    const int tx = threadIdx.x, ty = threadIdx.y;  // block (32, 8): rows ty + 8q
+    // phi rows k0 .. k0+32 (33 with the k+1 halo) of columns j0 .. j0+32
+    // (the last one periodic), all loads issued before the tile is written
+    {
+        double a0[5], a1[5], a2[5];
+        const int jc = j0 + tx;                  // column tx
+        const int jw = (jc == ny) ? 0 : jc;
+        const int jh = (j0 + 32 == ny) ? 0 : j0 + 32;  // column 32 (thread tx 0)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const int r = ty + 8 * q, k = k0 + r;
+            const bool row = r < 33 && k < nz;
+            const size_t b0 = ((size_t)k * nx + i) * ny, b1 = ((size_t)k * nx + i1) * ny;
+            a0[q] = (row && jc <= ny) ? phi[b0 + jw] : 0.0;
+            a1[q] = (row && r < 32 && jc <= ny) ? phi[b1 + jw] : 0.0;
+            a2[q] = (row && tx == 0 && j0 + 32 <= ny) ? phi[b0 + jh] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const int r = ty + 8 * q;
+            if (r < 33) {
+                t0[r][tx] = a0[q];
+                if (r < 32) t1[r][tx] = a1[q];
+                if (tx == 0) t0[r][32] = a2[q];
+            }
         }
     }
     __syncthreads();
@@ -316,18 +335,33 @@ __device__ __forceinline__ void project_tile(const SlcParams &P, const double *_
     const size_t vsx = (size_t)(ny + 1) * (nz + 2), vsy = nz + 2;
     const size_t wsx = (size_t)(ny + 2) * (nz + 1), wsy = nz + 1;
     const size_t psx = (size_t)(ny + 2) * (nz + 2), psy = nz + 2;
-    for (int r = ty; r < 32; r += 8) {
-        const int j = j0 + r, k = k0 + tx;
+    // the four rows' velocity loads are issued before any update is stored
+    const int k = k0 + tx;
+    const size_t I = i + 1, K = k + 1;
+    double uo[4], vo[4], wo[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = j0 + ty + 8 * q;
+        const bool in = j < ny && k < nz;
+        const size_t J = j + 1;
+        uo[q] = in ? u[I * usx + J * usy + K] : 0.0;
+        vo[q] = in ? v[I * vsx + J * vsy + K] : 0.0;
+        wo[q] = (in && k < nz - 1) ? w[I * wsx + J * wsy + K] : 0.0;
+    }
+    const double rdz = (k < nz - 1) ? dz_c[k + 1] : 1.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int r = ty + 8 * q, j = j0 + r;
         if (j >= ny || k >= nz) continue;
         const double f0 = t0[tx][r];
         const double fx = t1[tx][r];
         const double fy = t0[tx][r + 1];
-        const size_t I = i + 1, J = j + 1, K = k + 1;
-        u[I * usx + J * usy + K] -= dt * ((fx - f0) * P.inv_dx);
-        v[I * vsx + J * vsy + K] -= dt * ((fy - f0) * P.inv_dy);
+        const size_t J = j + 1;
+        u[I * usx + J * usy + K] = uo[q] - dt * ((fx - f0) * P.inv_dx);
+        v[I * vsx + J * vsy + K] = vo[q] - dt * ((fy - f0) * P.inv_dy);
         if (k < nz - 1) {
             const double fz = t0[tx + 1][r];
-            w[I * wsx + J * wsy + K] -= dt * ((fz - f0) / dz_c[k + 1]);
+            w[I * wsx + J * wsy + K] = wo[q] - dt * ((fz - f0) / rdz);
         }
         p[I * psx + J * psy + K] = f0;
     }
