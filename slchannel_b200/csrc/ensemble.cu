@@ -189,11 +189,11 @@ void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
     }
     end(e->r_div);
     e->r_pr = e->r_div;
-    // Poisson Thomas sweep: 2 threads per (kx, ky) column, 256 per block
+    // Poisson Thomas sweep: 4 threads per (kx, ky) column, 256 per block
     begin(e->r_th);
     for (int i = 0; i < n; ++i) {
         const SlcParams &P = e->grids[i]->P;
-        const long long nthr = 2LL * P.nx * (P.ny / 2 + 1);
+        const long long nthr = 4LL * P.nx * (P.ny / 2 + 1);
         const int nb = (int)((nthr + 255) / 256);
         for (int b = 0; b < nb; ++b) items.push_back({i, b, 0, 0});
     }

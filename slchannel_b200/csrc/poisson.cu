@@ -192,6 +192,40 @@ __global__ void k_divergence(SlcParams P, const double *__restrict__ u,
 
 constexpr int kPre = 8;  // loads kept in flight per thread in the sweeps
 
+// Row k of the (kx, ky) column's system: sub-diagonal a, diagonal b,
+// super-diagonal c (projection.py:47-114), Neumann rows folded into b; the
+// (0, 0) mode's first row is the identity (projection.py:113-114).
+struct Row3 {
+    double a, b, c;
+};
+
+__device__ __forceinline__ Row3 poisson_row(const double *__restrict__ cl,
+                                            const double *__restrict__ cr, double k2, int nz, int k,
+                                            bool pinned)
+{
+    Row3 r;
+    r.a = k > 0 ? cl[k] : 0.0;
+    r.b = -(cl[k] + cr[k] + k2);
+    if (k == 0) r.b += cl[0];
+    if (k == nz - 1) r.b += cr[nz - 1];
+    r.c = k < nz - 1 ? cr[k] : 0.0;
+    if (pinned && k == 0) {
+        r.b = 1.0;
+        r.c = 0.0;
+    }
+    return r;
+}
+
+// Twisted (two-ended) Thomas elimination: four threads per column, part (re /
+// im) x half.  Half 0 eliminates rows 0 .. m-1 downwards as the reference's
+// Thomas sweep does; half 1 eliminates rows nz-1 .. m+1 upwards (sub- and
+// super-diagonal exchanged); the two meet at row m = nz/2, which the adjacent
+// lanes solve from each other's last pivot row (one shuffle), then each back-
+// substitutes its half.  Twice the threads of a one-ended sweep in flight for
+// the same arithmetic; the meeting row changes results by rounding only.  The
+// coefficients are real, so the real and imaginary parts are independent
+// systems; the part-0 thread of each half stores the pivot ratios g (same
+// values for both parts), read back by both after a warp barrier.
 __device__ __forceinline__ void thomas_column(const SlcParams &P, double *__restrict__ hat,
                                               double *__restrict__ cpw,
                                               const double *__restrict__ kx2,
@@ -199,15 +233,11 @@ __device__ __forceinline__ void thomas_column(const SlcParams &P, double *__rest
                                               const double *__restrict__ cl,
                                               const double *__restrict__ cr, double norm, int t)
 {
-    // thread t handles part (t & 1) (0 real, 1 imaginary) of column t >> 1; the
-    // coefficients are real, so the two parts are independent systems.  The
-    // real-part thread stores c' (same values in both), read back by both after
-    // a warp barrier.
     const int nky = P.ny / 2 + 1;
     const int ncol = P.nx * nky;
-    const int col = t >> 1, part = t & 1;
+    const int col = t >> 2, part = (t >> 1) & 1, half = t & 1;
     const bool active = col < ncol;
-    const int nz = P.nz;
+    const int nz = P.nz, m = nz / 2;
     const size_t st = 2 * (size_t)ncol;  // doubles per k-plane of the spectrum
     double *h = hat + 2 * (size_t)(active ? col : 0) + part;
     double *cpc = cpw + (active ? col : 0);
@@ -216,61 +246,67 @@ __device__ __forceinline__ void thomas_column(const SlcParams &P, double *__rest
         const int kx = col / nky, ky = col - (col / nky) * nky;
         k2 = kx2[kx] + ky2[ky];
     }
+    const bool pinned = active && col == 0;
+    const int cnt = active ? (half ? nz - 1 - m : m) : 0;  // rows this thread eliminates
+    // row of elimination step q: downwards from 0, or upwards from nz-1
+#define TH_ROW(q) (half ? nz - 1 - (q) : (q))
     double buf[kPre];
-    if (active) {
 #pragma unroll
-        for (int q = 0; q < kPre; ++q) buf[q] = q < nz ? h[q * st] : 0.0;
-        double cprev = 0.0, dprev = 0.0;
-        for (int k0 = 0; k0 < nz; k0 += kPre) {
+    for (int q = 0; q < kPre; ++q) buf[q] = q < cnt ? h[TH_ROW(q) * st] : 0.0;
+    double gprev = 0.0, dprev = 0.0;
+    for (int q0 = 0; q0 < cnt; q0 += kPre) {
 #pragma unroll
-            for (int q = 0; q < kPre; ++q) {
-                const int k = k0 + q;
-                if (k < nz) {
-                    const double d = buf[q];
-                    if (k + kPre < nz) buf[q] = h[(k + kPre) * st];
-                    const double a = k > 0 ? cl[k] : 0.0;
-                    double b = -(cl[k] + cr[k] + k2);
-                    if (k == 0) b += cl[0];
-                    if (k == nz - 1) b += cr[nz - 1];
-                    double c = k < nz - 1 ? cr[k] : 0.0;
-                    if (col == 0 && k == 0) {  // pinned (0,0) mode: identity first row
-                        b = 1.0;
-                        c = 0.0;
-                    }
-                    const double id = 1.0 / (b - a * cprev);
-                    cprev = c * id;
-                    dprev = (d - a * dprev) * id;
-                    h[k * st] = dprev;
-                    if (part == 0) cpc[k * (size_t)ncol] = cprev;
-                }
+        for (int u = 0; u < kPre; ++u) {
+            const int q = q0 + u;
+            if (q < cnt) {
+                const int k = TH_ROW(q);
+                const double d = buf[u];
+                if (q + kPre < cnt) buf[u] = h[TH_ROW(q + kPre) * st];
+                const Row3 R = poisson_row(cl, cr, k2, nz, k, pinned);
+                const double e = half ? R.c : R.a, f = half ? R.a : R.c;
+                const double id = 1.0 / (R.b - e * gprev);
+                gprev = f * id;
+                dprev = (d - e * dprev) * id;
+                h[k * st] = dprev;
+                if (part == 0) cpc[k * (size_t)ncol] = gprev;
             }
         }
     }
-    __syncwarp();
-    if (active) {
-        // back substitution, prefetching d' and c' downwards
-        double cb[kPre];
+#undef TH_ROW
+    // the meeting row m from both halves' last pivot rows
+    const double og = __shfl_xor_sync(0xffffffffu, gprev, 1);
+    const double od = __shfl_xor_sync(0xffffffffu, dprev, 1);
+    __syncwarp();  // the pivot ratios stored above are visible to the whole warp
+    const double gt = half ? og : gprev, dtp = half ? od : dprev;  // row m-1 (top)
+    const double gb = half ? gprev : og, dbt = half ? dprev : od;  // row m+1 (bottom)
+    const Row3 R = poisson_row(cl, cr, k2, nz, m, pinned);
+    const double dm = active ? h[m * st] : 0.0;
+    const double xm = (dm - R.a * dtp - R.c * dbt) / (R.b - R.a * gt - R.c * gb);
+    // back substitution outwards from m, prefetching d and g
+    double cb[kPre];
 #pragma unroll
-        for (int q = 0; q < kPre; ++q) {
-            const int k = nz - 1 - q;
-            buf[q] = k >= 0 ? h[k * st] : 0.0;
-            cb[q] = k >= 0 ? cpc[k * (size_t)ncol] : 0.0;
-        }
-        double x = 0.0;
-        for (int r0 = 0; r0 < nz; r0 += kPre) {
+    for (int q = 0; q < kPre; ++q) {
+        const int k = half ? m + 1 + q : m - 1 - q;
+        buf[q] = q < cnt ? h[k * st] : 0.0;
+        cb[q] = q < cnt ? cpc[k * (size_t)ncol] : 0.0;
+    }
+    __syncwarp();  // every lane has read row m before the top half writes it
+    if (active && half == 0) h[m * st] = xm * norm;
+    double x = xm;
+    for (int q0 = 0; q0 < cnt; q0 += kPre) {
 #pragma unroll
-            for (int q = 0; q < kPre; ++q) {
-                const int k = nz - 1 - (r0 + q);
-                if (k >= 0) {
-                    const double dk = buf[q], ck = cb[q];
-                    const int kn = k - kPre;
-                    if (kn >= 0) {
-                        buf[q] = h[kn * st];
-                        cb[q] = cpc[kn * (size_t)ncol];
-                    }
-                    x = (k == nz - 1) ? dk : dk - ck * x;
-                    h[k * st] = x * norm;
+        for (int u = 0; u < kPre; ++u) {
+            const int q = q0 + u;
+            if (q < cnt) {
+                const int k = half ? m + 1 + q : m - 1 - q;
+                const double dk = buf[u], gk = cb[u];
+                if (q + kPre < cnt) {
+                    const int kn = half ? k + kPre : k - kPre;
+                    buf[u] = h[kn * st];
+                    cb[u] = cpc[kn * (size_t)ncol];
                 }
+                x = dk - gk * x;
+                h[k * st] = x * norm;
             }
         }
     }
@@ -612,7 +648,7 @@ cudaError_t launch_thomas_poisson(const SlcParams &P, double *hat, double *cp, c
                                   const double *ky2, const double *cl, const double *cr,
                                   cudaStream_t s)
 {
-    const long long nthr = 2LL * P.nx * (P.ny / 2 + 1);
+    const long long nthr = 4LL * P.nx * (P.ny / 2 + 1);  // thomas_column: 4 per column
     const double norm = 1.0 / ((double)P.nx * (double)P.ny);
     k_thomas<<<(unsigned)((nthr + 255) / 256), 256, 0, s>>>(P, hat, cp, kx2, ky2, cl, cr, norm);
     count_launches(1);
