@@ -41,6 +41,7 @@ struct slc_ensemble {
     } r_bc, r_lin, r_sl, r_zs, r_div, r_th, r_pr, r_bulk, r_pp, r_pack;
     int max_ch = 1;
     int sl_grid = 148;
+    int pack_threads = 32;  // k_pack_mixed_ens block size: the largest instance's levels
     // FFT groups (instances sharing nx, ny): pools and plans
     struct Group {
         int nx = 0, ny = 0, planes = 0;
@@ -128,6 +129,7 @@ void free_groups(slc_ensemble *e)
 void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
 {
     items.clear();
+    e->pack_threads = 32;
     const int n = (int)e->grids.size();
     auto begin = [&](slc_ensemble::Range &r) { r.off = (int)items.size(); };
     auto end = [&](slc_ensemble::Range &r) { r.n = (int)items.size() - r.off; };
@@ -215,10 +217,11 @@ void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
         for (int i = 0; i < n; ++i) {
             const SlcParams &P = e->grids[i]->P;
             const MixedWS &ws = e->grids[i]->mws;
-            const int nzp = std::max(ws.nzp[0], ws.nzp[2]);
+            e->pack_threads = std::max(e->pack_threads,
+                                       mixed_pack_threads(std::max(ws.nzp[0], ws.nzp[2])));
+            const int nj = (P.ny + mixed_pack_cols() - 1) / mixed_pack_cols();
             for (int z = 0; z < 3 * P.nx; ++z)
-                for (int y = 0; y < P.ny; ++y)
-                    for (int x = 0; x < (nzp + 127) / 128; ++x) items.push_back({i, x, y, z});
+                for (int jb = 0; jb < nj; ++jb) items.push_back({i, jb, z, 0});
         }
     end(e->r_pack);
 }
@@ -257,7 +260,7 @@ int enqueue_step(slc_ensemble *e, int ph, cudaStream_t s)
     ENS_CK(launch_bc_ens(I, items_at(e, e->r_bc), e->r_bc.n, cur, 0, s), "boundary conditions");
     if (e->mixed)
         ENS_CK(launch_mixed_prepare_ens(I, n, items_at(e, e->r_pp), e->r_pp.n, items_at(e, e->r_pack),
-                                        e->r_pack.n, ph, s),
+                                        e->r_pack.n, e->pack_threads, ph, s),
                "mixed-form means and packs");
     else
         ENS_CK(launch_lincomb_ens(I, items_at(e, e->r_lin), e->r_lin.n, ph, s), "U* = 2V^n - V^{n-1}");
@@ -551,7 +554,7 @@ int slc_ensemble_autotune(slc_ensemble *e, int phase, int reps, int *tkl_out, do
     ENS_CK(launch_bc_ens(e->d_inst, items_at(e, e->r_bc), e->r_bc.n, ens_cur(phase), 0, s), "bc");
     if (e->mixed)
         ENS_CK(launch_mixed_prepare_ens(e->d_inst, n, items_at(e, e->r_pp), e->r_pp.n, items_at(e, e->r_pack),
-                                        e->r_pack.n, phase, s),
+                                        e->r_pack.n, e->pack_threads, phase, s),
                "mixed prepare");
     else
         ENS_CK(launch_lincomb_ens(e->d_inst, items_at(e, e->r_lin), e->r_lin.n, phase, s), "U*");

@@ -9,6 +9,8 @@
 // and everything after the predictor stay FP64.  The reference's counterpart
 // is its 'fp32_accum64' path (semilag.py:249-256, semilag_triton.py), which
 // runs the whole interpolation in FP32 instead.
+#include <algorithm>
+
 #include "slc_internal.h"
 
 namespace {
@@ -320,8 +322,9 @@ __global__ void __launch_bounds__(kThreads, 2)
 
 // ---- plane means -----------------------------------------------------------
 // Field f of `srcs` (component comp[f], ghost-shaped FP64): block (b, f) sums
-// the node columns b, b + G, ... level by level (threads over k, coalesced)
-// into partials[(f * G + b) * ldp + k].  Fixed order: bit-reproducible.
+// the b-th of G contiguous ranges of node columns level by level (threads
+// over k, coalesced) into partials[(f * G + b) * ldp + k].  Fixed order:
+// bit-reproducible.
 struct MeanSrcs {
     const double *p[9];
     int comp[9];
@@ -332,29 +335,46 @@ __device__ __forceinline__ void plane_partial(const SlcParams &P, const double *
 {
     const int NZ = C == 2 ? P.nz + 1 : P.nz + 2;
     const NodeView<double> V = ghost_view<double>(C, src, P.nx, P.ny, P.nz);
-    constexpr int kMaxPer = 5;  // NZ <= 1026 levels over 256 threads
+    constexpr int kMaxPer = 5;  // levels per thread: NZ <= 5 blockDim.x
     double acc[kMaxPer];
 #pragma unroll
     for (int q = 0; q < kMaxPer; ++q) acc[q] = 0.0;
+    // block b sums the contiguous column range [c0, c1), eight adjacent
+    // columns' loads in flight, added in column order
     const int ncol = P.nx * P.ny;
-    for (int col = b; col < ncol; col += G) {
-        const int i = col / P.ny, j = col - (col / P.ny) * P.ny;
-        const double *c = V.p + (size_t)i * V.sx + (size_t)j * V.sy;
+    const int c0 = (int)(((long long)ncol * b) / G), c1 = (int)(((long long)ncol * (b + 1)) / G);
+    constexpr int kCols = 8;
+    for (int col0 = c0; col0 < c1; col0 += kCols) {
+        const int i0 = col0 / P.ny, j0 = col0 - i0 * P.ny;
 #pragma unroll
         for (int q = 0; q < kMaxPer; ++q) {
-            const int k = threadIdx.x + q * 256;
-            if (k < NZ) acc[q] += __ldg(c + k);
+            const int k = threadIdx.x + q * blockDim.x;
+            if (k < NZ) {
+                double val[kCols];
+                int i = i0, j = j0;
+#pragma unroll
+                for (int r = 0; r < kCols; ++r) {
+                    val[r] = (col0 + r < c1) ? __ldg(V.p + (size_t)i * V.sx + (size_t)j * V.sy + k) : 0.0;
+                    if (++j == P.ny) {
+                        j = 0;
+                        ++i;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kCols; ++r)
+                    if (col0 + r < c1) acc[q] += val[r];
+            }
         }
     }
     double *out = partials + ((size_t)f * G + b) * ldp;
 #pragma unroll
     for (int q = 0; q < kMaxPer; ++q) {
-        const int k = threadIdx.x + q * 256;
+        const int k = threadIdx.x + q * blockDim.x;
         if (k < NZ) out[k] = acc[q];
     }
 }
 
-__global__ void __launch_bounds__(256) k_plane_partials(SlcParams P, const __grid_constant__ MeanSrcs S, double *partials,
+__global__ void __launch_bounds__(1024) k_plane_partials(SlcParams P, const __grid_constant__ MeanSrcs S, double *partials,
                                                         int ldp)
 {
     const int f = blockIdx.y;
@@ -369,35 +389,45 @@ struct MeanPtrs {
 };
 
 __device__ __forceinline__ void plane_finish(const SlcParams &P, int nf, const double *partials,
-                                             int ldp, int G, const MeanPtrs &out, int derived_star,
-                                             int f)
+                                             int ldp, int G, double *mean, float *mean32,
+                                             int derived_star, int f)
 {
     const int NZ = (f % 3) == 2 ? P.nz + 1 : P.nz + 2;
     const double inv = 1.0 / ((double)P.nx * (double)P.ny);
+    // sums over the G column groups in group order, eight groups' loads in flight
+    auto group_sum = [&](int fs, int k) {
+        constexpr int kU = 8;
+        const double *p = partials + (size_t)fs * G * ldp + k;
+        double s = 0.0;
+        for (int b0 = 0; b0 < G; b0 += kU) {
+            double v[kU];
+#pragma unroll
+            for (int r = 0; r < kU; ++r) v[r] = (b0 + r < G) ? p[(size_t)(b0 + r) * ldp] : 0.0;
+#pragma unroll
+            for (int r = 0; r < kU; ++r)
+                if (b0 + r < G) s += v[r];
+        }
+        return s;
+    };
     for (int k = threadIdx.x; k < NZ; k += blockDim.x) {
         double m;
         if (f >= 6 && derived_star) {
-            double sa = 0.0, sb = 0.0;
-            for (int b = 0; b < G; ++b) {
-                sa += partials[((size_t)(f - 6) * G + b) * ldp + k];
-                sb += partials[((size_t)(f - 3) * G + b) * ldp + k];
-            }
+            const double sa = group_sum(f - 6, k), sb = group_sum(f - 3, k);
             m = 2.0 * (sa * inv) - sb * inv;
         } else {
             if (f >= nf) return;
-            double s = 0.0;
-            for (int b = 0; b < G; ++b) s += partials[((size_t)f * G + b) * ldp + k];
-            m = s * inv;
+            m = group_sum(f, k) * inv;
         }
-        out.m[f][k] = m;
-        out.m32[f][k] = (float)m;
+        mean[k] = m;
+        mean32[k] = (float)m;
     }
 }
 
 __global__ void k_plane_finish(SlcParams P, int nf, const double *partials, int ldp, int G,
-                               MeanPtrs out, int derived_star)
+                               const __grid_constant__ MeanPtrs out, int derived_star)
 {
-    plane_finish(P, nf, partials, ldp, G, out, derived_star, blockIdx.x);
+    plane_finish(P, nf, partials, ldp, G, out.m[blockIdx.x], out.m32[blockIdx.x], derived_star,
+                 blockIdx.x);
 }
 
 // FP32 fluctuation node buffers: field slot q = comp (0..2) + 3 * which
@@ -409,41 +439,74 @@ struct PackArgs {
     int nzp[3];
 };
 
-__device__ __forceinline__ void pack_mixed(const SlcParams &P, const PackArgs &a, int bx, int by,
-                                           int bz)
+// One thread per level (blockDim.x >= NZp, or a loop over levels) over kPackJ
+// adjacent columns (i, jb kPackJ + q) of component comp; the columns' loads
+// are issued before any store.
+constexpr int kPackJ = 4;
+
+// One component's sources and destinations, resolved by the caller.
+struct PackOne {
+    const double *A, *B, *M;           // ghost-shaped; M null: U* = 2A - B
+    float *fa, *fb, *fm;               // node buffers, NZp levels per column
+    const double *ma, *mb, *mm;        // plane means
+    int NZp;
+};
+
+__device__ __forceinline__ void pack_mixed(const SlcParams &P, const PackOne &a, int comp, int i,
+                                           int jb)
 {
-    const int comp = bz / P.nx, i = bz - comp * P.nx;
-    const int j = by;
-    const int k = bx * 128 + threadIdx.x;
     const int NZ = comp == 2 ? P.nz + 1 : P.nz + 2;
-    const int NZp = a.nzp[comp];
-    if (k >= NZp) return;
-    const size_t o = ((size_t)i * P.ny + j) * NZp + k;
-    if (k >= NZ) {
-        a.f32[comp][o] = 0.f;
-        a.f32[comp + 3][o] = 0.f;
-        a.f32[comp + 6][o] = 0.f;
-        return;
+    const int NZp = a.NZp;
+    const NodeView<double> VA = ghost_view<double>(comp, a.A, P.nx, P.ny, P.nz);
+    const NodeView<double> VB = ghost_view<double>(comp, a.B, P.nx, P.ny, P.nz);
+    const double *pm = a.M ? ghost_view<double>(comp, a.M, P.nx, P.ny, P.nz).p : nullptr;
+    for (int k = threadIdx.x; k < NZp; k += blockDim.x) {
+        const bool in = k < NZ;
+        const double ma = in ? a.ma[k] : 0.0, mb = in ? a.mb[k] : 0.0, mm = in ? a.mm[k] : 0.0;
+        double va[kPackJ], vb[kPackJ], vm[kPackJ];
+#pragma unroll
+        for (int q = 0; q < kPackJ; ++q) {
+            const int j = jb * kPackJ + q;
+            const bool ok = in && j < P.ny;
+            const size_t n = (size_t)i * VA.sx + (size_t)j * VA.sy + k;
+            va[q] = ok ? VA.p[n] : 0.0;
+            vb[q] = ok ? VB.p[n] : 0.0;
+            vm[q] = (ok && pm) ? pm[n] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kPackJ; ++q) {
+            const int j = jb * kPackJ + q;
+            if (j >= P.ny) continue;
+            const size_t o = ((size_t)i * P.ny + j) * NZp + k;
+            if (!in) {  // padding levels
+                a.fa[o] = 0.f;
+                a.fb[o] = 0.f;
+                a.fm[o] = 0.f;
+                continue;
+            }
+            const double m = pm ? vm[q] : 2.0 * va[q] - vb[q];
+            a.fa[o] = (float)(va[q] - ma);
+            a.fb[o] = (float)(vb[q] - mb);
+            a.fm[o] = (float)(m - mm);
+        }
     }
-    const NodeView<double> VA = ghost_view<double>(comp, a.A[comp], P.nx, P.ny, P.nz);
-    const NodeView<double> VB = ghost_view<double>(comp, a.B[comp], P.nx, P.ny, P.nz);
-    const size_t n = (size_t)i * VA.sx + (size_t)j * VA.sy + k;
-    const double va = VA.p[n], vb = VB.p[n];
-    double vm;
-    if (a.M[comp]) {
-        const NodeView<double> VM = ghost_view<double>(comp, a.M[comp], P.nx, P.ny, P.nz);
-        vm = VM.p[n];
-    } else {
-        vm = 2.0 * va - vb;
-    }
-    a.f32[comp][o] = (float)(va - a.mean[comp][k]);
-    a.f32[comp + 3][o] = (float)(vb - a.mean[comp + 3][k]);
-    a.f32[comp + 6][o] = (float)(vm - a.mean[comp + 6][k]);
 }
 
-__global__ void __launch_bounds__(128) k_pack_mixed(SlcParams P, PackArgs a)
+__global__ void __launch_bounds__(1024) k_pack_mixed(SlcParams P, const __grid_constant__ PackArgs a)
 {
-    pack_mixed(P, a, blockIdx.x, blockIdx.y, blockIdx.z);
+    const int comp = blockIdx.y / P.nx, i = blockIdx.y - comp * P.nx;
+    PackOne o;
+    o.A = a.A[comp];
+    o.B = a.B[comp];
+    o.M = a.M[comp];
+    o.fa = a.f32[comp];
+    o.fb = a.f32[comp + 3];
+    o.fm = a.f32[comp + 6];
+    o.ma = a.mean[comp];
+    o.mb = a.mean[comp + 3];
+    o.mm = a.mean[comp + 6];
+    o.NZp = a.nzp[comp];
+    pack_mixed(P, o, comp, i, blockIdx.x);
 }
 
 // ---- ensemble forms (one launch per substep over all instances) ----
@@ -473,32 +536,29 @@ __global__ void k_plane_finish_ens(const EnsInst *__restrict__ ins)
 {
     const EnsInst &I = ins[blockIdx.x / 9];
     const int f = blockIdx.x % 9;
-    MeanPtrs mp;
-    for (int q = 0; q < 9; ++q) {
-        mp.m[q] = I.mws.mean[q];
-        mp.m32[q] = I.mws.mean32[q];
-    }
-    plane_finish(I.P, 6, I.mws.partials, I.P.nz + 2, kMeanBlocks, mp, 1, f);
+    plane_finish(I.P, 6, I.mws.partials, I.P.nz + 2, kMeanBlocks, I.mws.mean[f], I.mws.mean32[f], 1,
+                 f);
 }
 
 // items (inst, bx, by, bz) as k_pack_mixed's grid
-__global__ void __launch_bounds__(128) k_pack_mixed_ens(const EnsInst *__restrict__ ins,
+__global__ void __launch_bounds__(1024) k_pack_mixed_ens(const EnsInst *__restrict__ ins,
                                                         const EnsItem *__restrict__ items, int ph)
 {
     const EnsItem it = items[blockIdx.x];
     const EnsInst &I = ins[it.inst];
-    PackArgs a;
-    for (int c = 0; c < 3; ++c) {
-        a.A[c] = I.lev[ens_cur(ph)][c];
-        a.B[c] = I.lev[ens_prev(ph)][c];
-        a.M[c] = nullptr;
-        a.nzp[c] = I.mws.nzp[c];
-    }
-    for (int q = 0; q < 9; ++q) {
-        a.f32[q] = I.mws.f32[q];
-        a.mean[q] = I.mws.mean[q];
-    }
-    pack_mixed(I.P, a, it.a, it.b, it.c);
+    const int comp = it.b / I.P.nx, i = it.b - comp * I.P.nx;
+    PackOne o;
+    o.A = I.lev[ens_cur(ph)][comp];
+    o.B = I.lev[ens_prev(ph)][comp];
+    o.M = nullptr;
+    o.fa = I.mws.f32[comp];
+    o.fb = I.mws.f32[comp + 3];
+    o.fm = I.mws.f32[comp + 6];
+    o.ma = I.mws.mean[comp];
+    o.mb = I.mws.mean[comp + 3];
+    o.mm = I.mws.mean[comp + 6];
+    o.NZp = I.mws.nzp[comp];
+    pack_mixed(I.P, o, comp, i, it.a);
 }
 
 // Persistent mixed-form BDF2 trace+gather over the (instance, component, x
@@ -587,7 +647,10 @@ cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const 
         S.comp[f] = f % 3;
     }
     const int ldp = P.nz + 2;
-    k_plane_partials<<<dim3(kMeanBlocks, nf), 256, 0, s>>>(P, S, ws.partials, ldp);
+    // one thread per level (a warp covering the last few levels alone would
+    // make a second dependent round of loads the block's critical path)
+    const int pt = std::min(1024, (P.nz + 2 + 31) / 32 * 32);
+    k_plane_partials<<<dim3(kMeanBlocks, nf), pt, 0, s>>>(P, S, ws.partials, ldp);
     MeanPtrs mp;
     for (int f = 0; f < 9; ++f) {
         mp.m[f] = ws.mean[f];
@@ -606,7 +669,7 @@ cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const 
         a.mean[q] = ws.mean[q];
     }
     const int nzp_max = ws.nzp[0] > ws.nzp[2] ? ws.nzp[0] : ws.nzp[2];
-    k_pack_mixed<<<dim3((nzp_max + 127) / 128, P.ny, 3 * P.nx), 128, 0, s>>>(P, a);
+    k_pack_mixed<<<dim3((P.ny + kPackJ - 1) / kPackJ, 3 * P.nx), mixed_pack_threads(nzp_max), 0, s>>>(P, a);
     count_launches(3);
     return cudaGetLastError();
 }
@@ -627,14 +690,17 @@ cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, cons
 }
 
 int mixed_mean_blocks() { return kMeanBlocks; }
+int mixed_pack_cols() { return kPackJ; }
+int mixed_pack_threads(int nzp) { return std::min(1024, (nzp + 31) / 32 * 32); }
 
 cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsItem *pp_items, int n_pp,
-                                     const EnsItem *pack_items, int n_pack, int ph, cudaStream_t s)
+                                     const EnsItem *pack_items, int n_pack, int pack_threads, int ph,
+                                     cudaStream_t s)
 {
     if (ninst <= 0) return cudaSuccess;
     k_plane_partials_ens<<<n_pp, 256, 0, s>>>(ins, pp_items, ph);
     k_plane_finish_ens<<<9 * ninst, 256, 0, s>>>(ins);
-    k_pack_mixed_ens<<<n_pack, 128, 0, s>>>(ins, pack_items, ph);
+    k_pack_mixed_ens<<<n_pack, pack_threads, 0, s>>>(ins, pack_items, ph);
     count_launches(3);
     return cudaGetLastError();
 }

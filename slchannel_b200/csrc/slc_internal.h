@@ -186,7 +186,10 @@ cudaError_t launch_sl_tma(const SlcParams &P, Tri fn, Tri fnm1, Tri mid, double 
 // packs (items (inst, bx, by, bz) of k_pack_mixed's grid), and the
 // persistent trace+gather.
 int mixed_mean_blocks();
+int mixed_pack_cols();              // y columns one k_pack_mixed block covers
+int mixed_pack_threads(int nzp);     // its block size for nzp padded levels
 cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsItem *pp_items, int n_pp,
-                                     const EnsItem *pack_items, int n_pack, int ph, cudaStream_t s);
+                                     const EnsItem *pack_items, int n_pack, int pack_threads, int ph,
+                                     cudaStream_t s);
 cudaError_t launch_sl_mixed_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
                                 unsigned *queue, int grid, cudaStream_t s);
