@@ -345,7 +345,7 @@ int slc_ensemble_create(const slc_grid_desc *descs, int n, slc_ensemble **out)
     }
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e->device);
-    e->sl_grid = dev_sms * sl_ens_blocks_per_sm();
+    e->sl_grid = dev_sms * (e->mixed ? sl_mixed_ens_blocks_per_sm() : sl_ens_blocks_per_sm());
     *out = e;
     return SLC_OK;
 }

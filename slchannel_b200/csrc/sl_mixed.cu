@@ -17,6 +17,13 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kTileK = 64, kTileJ = kThreads / kTileK;
+// resident blocks per SM the mixed trace+gather kernel is compiled for
+#ifndef SLC_SLM_MIN_BLOCKS
+#define SLC_SLM_MIN_BLOCKS 4
+#endif
+#ifndef SLC_SLM_ENS_MIN_BLOCKS  // the persistent ensemble form (more live state)
+#define SLC_SLM_ENS_MIN_BLOCKS 3
+#endif
 constexpr int kMeanBlocks = 148;  // column groups of the plane-mean partial sums
 
 struct Vel3M {
@@ -307,8 +314,10 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
 }
 
 template <int C, int O, int MODE>
-__global__ void __launch_bounds__(kThreads, 2)
-    k_sl_mixed(SlcParams P, Vel3M M, MixedView FA, MixedView FB, const double *__restrict__ fn,
+__global__ void __launch_bounds__(kThreads, SLC_SLM_MIN_BLOCKS)
+    k_sl_mixed(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3M M,
+               const __grid_constant__ MixedView FA, const __grid_constant__ MixedView FB,
+               const double *__restrict__ fn,
                const double *__restrict__ fnm1, double dt, double *__restrict__ out,
                unsigned long long *nclamp)
 {
@@ -564,7 +573,7 @@ __global__ void __launch_bounds__(1024) k_pack_mixed_ens(const EnsInst *__restri
 // Persistent mixed-form BDF2 trace+gather over the (instance, component, x
 // index, tile) queue; the structure of the FP64 ensemble kernel.
 template <int O>
-__global__ void __launch_bounds__(kThreads, 2) k_sl_mixed_ens(const EnsInst *__restrict__ ins,
+__global__ void __launch_bounds__(kThreads, SLC_SLM_ENS_MIN_BLOCKS) k_sl_mixed_ens(const EnsInst *__restrict__ ins,
                                                               const EnsItem *__restrict__ items,
                                                               int nitems, int ph, unsigned *queue)
 {
@@ -690,6 +699,16 @@ cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, cons
 }
 
 int mixed_mean_blocks() { return kMeanBlocks; }
+
+int sl_mixed_ens_blocks_per_sm()
+{
+    int nb = 0, nb4 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sl_mixed_ens<6>, kThreads, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb4, k_sl_mixed_ens<4>, kThreads, 0) != cudaSuccess)
+        return 1;
+    const int m = nb < nb4 ? nb : nb4;
+    return m > 0 ? m : 1;
+}
 int mixed_pack_cols() { return kPackJ; }
 int mixed_pack_threads(int nzp) { return std::min(1024, (nzp + 31) / 32 * 32); }
 

@@ -18,6 +18,10 @@
 namespace {
 
 constexpr int kThreads = 256;
+// resident blocks per SM the trace+gather kernel is compiled for (register cap)
+#ifndef SLC_SL_MIN_BLOCKS
+#define SLC_SL_MIN_BLOCKS 2
+#endif
 
 #include "sl_device.cuh"
 
@@ -69,7 +73,7 @@ __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
 }
 
 template <int C, int O, int MODE, int TO>
-__global__ void __launch_bounds__(kThreads, 2) k_sl(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, const double *__restrict__ fn,
+__global__ void __launch_bounds__(kThreads, SLC_SL_MIN_BLOCKS) k_sl(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, const double *__restrict__ fn,
                                                     const double *__restrict__ fnm1, double dt,
                                                     double *__restrict__ out,
                                                     unsigned long long *nclamp)

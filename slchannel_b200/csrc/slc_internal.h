@@ -139,6 +139,7 @@ __host__ __device__ inline int ens_next(int ph) { return (ph + 2) % 3; }
 cudaError_t launch_sl_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
                           unsigned *queue, int grid, cudaStream_t s);
 int sl_ens_blocks_per_sm();
+int sl_mixed_ens_blocks_per_sm();  // resident blocks of the mixed persistent kernel
 // U* for every instance: items (inst, comp, chunk of 1024 elements).
 cudaError_t launch_lincomb_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph,
                                cudaStream_t s);
