@@ -138,6 +138,12 @@ SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *v
  * only, so feeding each call's next back as the following call's cur
  * pipelines the round trip.  Returns after enqueueing; the outputs are on the
  * host, and the host buffers may be touched again, once `stream` completes.
+ * The step computes on an internal stream of the handle: ordered after the
+ * handle's previous host-state call (and, at the first call, after work
+ * already enqueued on `stream`), not after later work of the caller's, so
+ * one call's compute overlaps the previous call's downloads.  Other entry
+ * points that use the same handle on another stream must be ordered by the
+ * caller (synchronise `stream` first).
  * No counterpart in the reference (its state is device- or CPU-resident). */
 SLC_API int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const double *const prev[3],
                                double *const next[3], double *p, double *bulk_out2, double U_bulk,

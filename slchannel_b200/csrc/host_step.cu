@@ -5,7 +5,10 @@
 // shift on the device, and downloads V^{n+1}, p and (u_bulk, forcing).  The
 // transfers are overlapped with each other and with compute:
 //  * two copy streams (host-to-device, device-to-host) run concurrently with
-//    the compute stream;
+//    an internal compute stream.  Compute runs there rather than on the
+//    caller's stream, which ends each call waiting for that call's downloads:
+//    the next call's compute then starts when its inputs are on the device,
+//    not when the previous call's p has reached the host;
 //  * the device state is double-buffered across calls, so the next call's
 //    uploads proceed while this call computes;
 //  * copies are cut into chunks with one event each.  An upload whose host
@@ -34,7 +37,9 @@ struct Pending {
 
 struct HostStep {
     int device = 0;
-    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaStream_t h2d = nullptr, d2h = nullptr, comp = nullptr;
+    cudaEvent_t entry = nullptr;  // the caller's stream at the first call
+    bool started = false;
     double *dev[2][10] = {};  // set -> cur(3), prev(3), next(3), p
     double *scal2[2] = {nullptr, nullptr};
     cudaEvent_t inputs_ready[2] = {}, compute_done[2] = {}, set_free[2] = {};
@@ -99,6 +104,8 @@ int ensure_host_step(slc_grid *g)
     g->host = h;
     HS_CK(cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking), "copy stream");
     HS_CK(cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking), "copy stream");
+    HS_CK(cudaStreamCreateWithFlags(&h->comp, cudaStreamNonBlocking), "compute stream");
+    HS_CK(cudaEventCreateWithFlags(&h->entry, cudaEventDisableTiming), "event");
     for (int s = 0; s < 2; ++s) {
         for (int q = 0; q < 10; ++q) {
             const size_t n = q == 9 ? g->ghost_elems[3] : g->ghost_elems[q % 3];
@@ -126,6 +133,8 @@ void host_step_free(HostStep *h)
     if (!h) return;
     if (h->h2d) cudaStreamDestroy(h->h2d);
     if (h->d2h) cudaStreamDestroy(h->d2h);
+    if (h->comp) cudaStreamDestroy(h->comp);
+    if (h->entry) cudaEventDestroy(h->entry);
     for (int s = 0; s < 2; ++s) {
         if (h->inputs_ready[s]) cudaEventDestroy(h->inputs_ready[s]);
         if (h->compute_done[s]) cudaEventDestroy(h->compute_done[s]);
@@ -156,6 +165,12 @@ extern "C" int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const
     if (rc) return rc;
     HostStep *h = g->host;
     cudaStream_t s = (cudaStream_t)stream;
+    if (!h->started) {  // order the first call after the caller's earlier work on the handle
+        HS_CK(cudaEventRecord(h->entry, s), "record");
+        HS_CK(cudaStreamWaitEvent(h->comp, h->entry, 0), "wait caller");
+        HS_CK(cudaStreamWaitEvent(h->h2d, h->entry, 0), "wait caller");
+        h->started = true;
+    }
     const int set = h->set;
     double *const *D = h->dev[set];
     h->parity ^= 1;  // this call's events: the pool of two calls ago (no longer waited on)
@@ -189,13 +204,13 @@ extern "C" int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const
     }
     HS_CK(cudaEventRecord(h->inputs_ready[set], h->h2d), "record");
 
-    // compute on the caller's stream
-    HS_CK(cudaStreamWaitEvent(s, h->inputs_ready[set], 0), "wait inputs");
+    // compute on the internal stream, after the previous call's compute
+    HS_CK(cudaStreamWaitEvent(h->comp, h->inputs_ready[set], 0), "wait inputs");
     double *c3[3] = {D[0], D[1], D[2]}, *p3[3] = {D[3], D[4], D[5]}, *n3[3] = {D[6], D[7], D[8]};
-    rc = slc_step_bdf2(g, c3, p3, n3, D[9], dt, nullptr, stream);
-    if (!rc) rc = slc_bulk_shift(g, D[6], D[7], D[8], U_bulk, dt, h->scal2[set], stream);
+    rc = slc_step_bdf2(g, c3, p3, n3, D[9], dt, nullptr, h->comp);
+    if (!rc) rc = slc_bulk_shift(g, D[6], D[7], D[8], U_bulk, dt, h->scal2[set], h->comp);
     if (rc) return rc;
-    HS_CK(cudaEventRecord(h->compute_done[set], s), "record");
+    HS_CK(cudaEventRecord(h->compute_done[set], h->comp), "record");
 
     // downloads: V^{n+1} (the next call's input, first), (u_bulk, forcing),
     // then p; each after any upload still reading its host range
