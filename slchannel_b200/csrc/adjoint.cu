@@ -90,17 +90,6 @@ __device__ __forceinline__ void ubasis_all(const SlcParams &P, double t, double 
 }
 
 template <int O>
-__device__ __forceinline__ double zbasis(const double *zn, const double *dinv, int rows, int k0,
-                                         double z, int m)
-{
-    double pr = 1.0;
-#pragma unroll
-    for (int l = 0; l < O; ++l)
-        if (l != m) pr *= z - __ldg(zn + k0 + l);
-    return pr * __ldg(dinv + m * rows + k0);
-}
-
-template <int O>
 __device__ __forceinline__ void zbasis_all(const double *zn, const double *dinv, int rows, int k0, double z,
                                            double (&w)[O], double (&dw)[O])
 {
@@ -400,11 +389,10 @@ __global__ void __launch_bounds__(kT) k_sl_adj_points(SlcParams P, V3 M, const d
 }
 
 // ---- records -> (key, payload) -----------------------------------------------
-// Gather records of component C: key = (bx0 * ny + by0) * NZ + k0; payload
-// (tx, ty, z, coef).
+// Gather records (x, y, z, coef) of component C: key = (bx0 * ny + by0) * NZ + k0.
 template <int C, int O>
 __global__ void k_gather_keys(SlcParams P, const double4 *__restrict__ rec, long long n,
-                              int *__restrict__ keys, double4 *__restrict__ pay)
+                              int *__restrict__ keys)
 {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
@@ -412,7 +400,36 @@ __global__ void k_gather_keys(SlcParams P, const double4 *__restrict__ rec, long
     const GBase<C, O> b = gather_base<C, O>(P, R.x, R.y, R.z);
     const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
     keys[r] = (b.bx0 * P.ny + b.by0) * NZ + b.k0;
-    pay[r] = make_double4(b.tx, b.ty, R.z, R.w);
+}
+
+// The sorted gather records' separable weights, node-major (SoA) in key order:
+// record p adds coef wx[mx] * wy[my] * wz[mz] to node base + (mx, my, mz), with
+// W[mx * n + p] = coef wx[mx], W[(O + my) * n + p] = wy[my],
+// W[(2 O + mz) * n + p] = wz[mz] (the forward gather's own weight functions)
+// and kz[p] its stencil's first z node.
+template <int C, int O>
+__global__ void __launch_bounds__(kT) k_sorted_weights(SlcParams P, const double4 *__restrict__ rec,
+                                                       const int *__restrict__ order, long long n,
+                                                       double *__restrict__ W, int *__restrict__ kz)
+{
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const double4 R = rec[__ldg(order + p)];
+    const GBase<C, O> b = gather_base<C, O>(P, R.x, R.y, R.z);
+    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
+    const double *zn = Comp<C>::centers ? P.zc : P.zf;
+    const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
+    double wx[O], wy[O], wz[O];
+    uniform_weights<O, double>(P, b.tx, wx);
+    uniform_weights<O, double>(P, b.ty, wy);
+    z_weights<O, double>(zn, dinv, NZ - O + 1, b.k0, R.z, wz);
+#pragma unroll
+    for (int m = 0; m < O; ++m) {
+        W[(size_t)m * n + p] = R.w * wx[m];
+        W[(size_t)(O + m) * n + p] = wy[m];
+        W[(size_t)(2 * O + m) * n + p] = wz[m];
+    }
+    kz[p] = b.k0;
 }
 
 // Trilinear records for field c of U*: payload (tx, ty, wz1, coef_c).
@@ -552,9 +569,15 @@ __global__ void k_sort_segments(const int *__restrict__ starts, long long nkeys,
 }
 
 // ---- pulls: every target node sums the records whose stencil covers it -----
+// For each (mx, my), the stencil starts covering node iz along z are the
+// consecutive keys k0 = iz - O + 1 .. iz, so their records are one contiguous
+// range of the sorted order: two starts loads per (mx, my), then four
+// coalesced loads per record (lanes are consecutive iz, their ranges shifted
+// by one key).  Records are summed in key order, then record id: a fixed
+// order, so the result is reproducible bit for bit.
 template <int C, int O>
-__global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double4 *__restrict__ pay,
-                                                    const int *__restrict__ order,
+__global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double *__restrict__ W,
+                                                    const int *__restrict__ kz, long long nrec,
                                                     const int *__restrict__ starts, double *lam)
 {
     const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
@@ -564,23 +587,21 @@ __global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double4 *
     const int iz = (int)(t % NZ);
     const int iy = (int)((t / NZ) % P.ny);
     const int ix = (int)(t / ((long long)NZ * P.ny));
-    const double *zn = Comp<C>::centers ? P.zc : P.zf;
-    const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
+    const int klo = max(iz - (O - 1), 0), khi = min(iz, NZ - O);
     double acc = 0.0;
-    for (int mx = 0; mx < O; ++mx) {
-        const int bx = wrapn(ix - mx, P.nx);
-        for (int my = 0; my < O; ++my) {
-            const int by = wrapn(iy - my, P.ny);
-            for (int mz = 0; mz < O; ++mz) {
-                const int k0 = iz - mz;
-                if (k0 < 0 || k0 > NZ - O) continue;
-                const int key = (bx * P.ny + by) * NZ + k0;
-                const int a = __ldg(starts + key), b = __ldg(starts + key + 1);
+    if (klo <= khi) {
+        for (int mx = 0; mx < O; ++mx) {
+            const int bx = wrapn(ix - mx, P.nx);
+            const double *cwx = W + (size_t)mx * nrec;
+            for (int my = 0; my < O; ++my) {
+                const int by = wrapn(iy - my, P.ny);
+                const double *wyv = W + (size_t)(O + my) * nrec;
+                const int kb = (bx * P.ny + by) * NZ;
+                const int a = __ldg(starts + kb + klo), b = __ldg(starts + kb + khi + 1);
                 for (int p = a; p < b; ++p) {
-                    const double4 R = pay[__ldg(order + p)];
-                    const double w = ubasis<O>(P, R.x, mx) * ubasis<O>(P, R.y, my) *
-                                     zbasis<O>(zn, dinv, NZ - O + 1, k0, R.z, mz);
-                    acc = fma(R.w, w, acc);
+                    const int mz = iz - __ldg(kz + p);
+                    const double wz = __ldg(W + (size_t)(2 * O + mz) * nrec + p);
+                    acc = fma(__ldg(cwx + p) * __ldg(wyv + p), wz, acc);
                 }
             }
         }
@@ -964,6 +985,8 @@ struct AdjWS {
     int *sums = nullptr, *total = nullptr;
     double *lam_mid[3] = {nullptr, nullptr, nullptr};
     double *scratch = nullptr, *partials = nullptr, *S = nullptr;
+    double *W = nullptr;  // sorted gather weights, 3 O arrays of n_c[0]
+    int *kz = nullptr;    // sorted gather records' first z node
 };
 
 namespace {
@@ -1019,6 +1042,8 @@ int ensure_adj(slc_grid *g)
     if (!rc) rc = adj_alloc(g, &w->scratch, (size_t)3 * plane * P.nz, "adjoint z-solve scratch");
     if (!rc) rc = adj_alloc(g, &w->partials, (size_t)kSumBlocks, "adjoint partials");
     if (!rc) rc = adj_alloc(g, &w->S, (size_t)1, "adjoint sum");
+    if (!rc) rc = adj_alloc(g, &w->W, (size_t)3 * SLC_MAX_ORDER * w->n_c[0], "adjoint gather weights");
+    if (!rc) rc = adj_alloc(g, &w->kz, (size_t)w->n_c[0], "adjoint gather z bases");
     if (rc) {
         delete w;
         return rc;
@@ -1073,16 +1098,23 @@ int sl_adjoint_t(slc_grid *g, AdjWS *w, const V3 &M, const double *const cur[3],
         for (int foot = 0; foot < (MODE == 2 ? 2 : 1); ++foot) {
             const double4 *rec = foot == 0 ? w->rec_near : w->rec_far;
             double *dst = foot == 0 ? lam_cur[C] : lam_prev[C];
-            if (C == 0) k_gather_keys<0, O><<<nblk(n), kT, 0, s>>>(P, rec, n, w->keys, w->pay);
-            else if (C == 1) k_gather_keys<1, O><<<nblk(n), kT, 0, s>>>(P, rec, n, w->keys, w->pay);
-            else k_gather_keys<2, O><<<nblk(n), kT, 0, s>>>(P, rec, n, w->keys, w->pay);
+            if (C == 0) k_gather_keys<0, O><<<nblk(n), kT, 0, s>>>(P, rec, n, w->keys);
+            else if (C == 1) k_gather_keys<1, O><<<nblk(n), kT, 0, s>>>(P, rec, n, w->keys);
+            else k_gather_keys<2, O><<<nblk(n), kT, 0, s>>>(P, rec, n, w->keys);
             count_launches(1);
             int rc = sort_records(g, w, n, nkeys, s);
             if (rc) return rc;
-            if (C == 0) k_pull_gather<0, O><<<nblk(nkeys), kT, 0, s>>>(P, w->pay, w->order, w->starts, dst);
-            else if (C == 1) k_pull_gather<1, O><<<nblk(nkeys), kT, 0, s>>>(P, w->pay, w->order, w->starts, dst);
-            else k_pull_gather<2, O><<<nblk(nkeys), kT, 0, s>>>(P, w->pay, w->order, w->starts, dst);
-            count_launches(1);
+            if (C == 0) {
+                k_sorted_weights<0, O><<<nblk(n), kT, 0, s>>>(P, rec, w->order, n, w->W, w->kz);
+                k_pull_gather<0, O><<<nblk(nkeys), kT, 0, s>>>(P, w->W, w->kz, n, w->starts, dst);
+            } else if (C == 1) {
+                k_sorted_weights<1, O><<<nblk(n), kT, 0, s>>>(P, rec, w->order, n, w->W, w->kz);
+                k_pull_gather<1, O><<<nblk(nkeys), kT, 0, s>>>(P, w->W, w->kz, n, w->starts, dst);
+            } else {
+                k_sorted_weights<2, O><<<nblk(n), kT, 0, s>>>(P, rec, w->order, n, w->W, w->kz);
+                k_pull_gather<2, O><<<nblk(nkeys), kT, 0, s>>>(P, w->W, w->kz, n, w->starts, dst);
+            }
+            count_launches(2);
         }
         // explicit x, y diffusion
         const double cc = MODE == 2 ? (P.xy_lagged ? (2.0 / 3.0) * dt : (4.0 / 3.0) * dt) : dt;

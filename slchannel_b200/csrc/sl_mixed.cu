@@ -16,7 +16,10 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kTileK = 64, kTileJ = kThreads / kTileK;
+#ifndef SLC_SLM_TILE_K
+#define SLC_SLM_TILE_K 32
+#endif
+constexpr int kTileK = SLC_SLM_TILE_K, kTileJ = kThreads / kTileK;
 // resident blocks per SM the mixed trace+gather kernel is compiled for
 #ifndef SLC_SLM_MIN_BLOCKS
 #define SLC_SLM_MIN_BLOCKS 4

@@ -30,7 +30,10 @@ constexpr int kThreads = 256;
 // MODE 2: BDF2 predictor 4/3 ubar - 1/3 ubarbar + (2/3)dt Rh (solver.py:846-903).
 // Launch geometry of k_sl: a block is kTileK consecutive z arrival points
 // (one warp each 32) x kTileJ y-rows at one x index; grid (z tiles, y tiles, nx).
-constexpr int kTileK = 64, kTileJ = kThreads / kTileK;
+#ifndef SLC_SL_TILE_K
+#define SLC_SL_TILE_K 64
+#endif
+constexpr int kTileK = SLC_SL_TILE_K, kTileJ = kThreads / kTileK;
 
 // One arrival point (i, j, k) of component C; out-of-range points only
 // contribute nothing.  Shared by the single-grid kernel below and the
