@@ -51,17 +51,6 @@ struct V3 {
 
 // ---- Lagrange basis values and derivatives ----------------------------------
 template <int O>
-__device__ __forceinline__ double ubasis(const SlcParams &P, double t, int m)
-{
-    constexpr int h = O / 2 - 1;
-    double pr = 1.0;
-#pragma unroll
-    for (int l = 0; l < O; ++l)
-        if (l != m) pr *= t - (double)(l - h);
-    return pr * P.udenom[O][m];
-}
-
-template <int O>
 __device__ __forceinline__ void ubasis_all(const SlcParams &P, double t, double (&w)[O],
                                            double (&dw)[O])
 {
