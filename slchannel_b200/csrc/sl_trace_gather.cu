@@ -22,6 +22,9 @@ constexpr int kThreads = 256;
 #ifndef SLC_SL_MIN_BLOCKS
 #define SLC_SL_MIN_BLOCKS 2
 #endif
+#ifndef SLC_SL_ENS_MIN_BLOCKS  // the persistent ensemble form
+#define SLC_SL_ENS_MIN_BLOCKS 2
+#endif
 
 #include "sl_device.cuh"
 
@@ -169,7 +172,7 @@ Vel3 make_vel(const SlcParams &P, Tri mid, bool node)
 // is sl_point's, so an instance's result does not depend on the tile shape
 // or on the other instances.
 template <int O>
-__global__ void __launch_bounds__(kThreads, 2) k_sl_ens(const EnsInst *__restrict__ ins,
+__global__ void __launch_bounds__(kThreads, SLC_SL_ENS_MIN_BLOCKS) k_sl_ens(const EnsInst *__restrict__ ins,
                                                         const EnsItem *__restrict__ items,
                                                         int nitems, int ph, unsigned *queue)
 {
