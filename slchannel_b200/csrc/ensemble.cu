@@ -38,8 +38,8 @@ struct slc_ensemble {
     // item ranges inside d_items
     struct Range {
         int off = 0, n = 0;
-    } r_bc, r_lin, r_sl, r_zs, r_div, r_th, r_pr, r_bulk, r_pp, r_pack;
-    int max_ch = 1;
+    } r_bc, r_lin, r_sl, r_div, r_th, r_pr, r_bulk, r_pp, r_pack;
+    Range r_zs[kZsChunks];  // z-solve items grouped by chunk size
     int sl_grid = 148;
     int pack_threads = 32;  // k_pack_mixed_ens block size: the largest instance's levels
     // FFT groups (instances sharing nx, ny): pools and plans
@@ -171,16 +171,19 @@ void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
         }
     }
     end(e->r_sl);
-    // z-solve: blocks of zsolve_ens_warps() columns
-    begin(e->r_zs);
-    for (int i = 0; i < n; ++i) {
-        const SlcParams &P = e->grids[i]->P;
-        const long long warps = 3LL * P.nx * P.ny;
-        const int W = zsolve_ens_warps();
-        const int nb = (int)((warps + W - 1) / W);
-        for (int b = 0; b < nb; ++b) items.push_back({i, b, 0, 0});
+    // z-solve: blocks of zsolve_ens_warps() columns, grouped by chunk size
+    for (int q = 0; q < kZsChunks; ++q) {
+        begin(e->r_zs[q]);
+        for (int i = 0; i < n; ++i) {
+            const SlcParams &P = e->grids[i]->P;
+            if (zsolve_chunk(P.nz) != kZsChunkValues[q]) continue;
+            const long long warps = 3LL * P.nx * P.ny;
+            const int W = zsolve_ens_warps();
+            const int nb = (int)((warps + W - 1) / W);
+            for (int b = 0; b < nb; ++b) items.push_back({i, b, 0, 0});
+        }
+        end(e->r_zs[q]);
     }
-    end(e->r_zs);
     // divergence pack and projection: 32 x 32 (k, j) tiles per x index
     begin(e->r_div);
     for (int i = 0; i < n; ++i) {
@@ -274,7 +277,9 @@ int enqueue_step(slc_ensemble *e, int ph, cudaStream_t s)
     else
         ENS_CK(launch_sl_ens(I, items_at(e, e->r_sl), e->r_sl.n, ph, e->order, e->d_queue, e->sl_grid, s),
                "trace+gather BDF2");
-    ENS_CK(launch_zsolve_ens(I, items_at(e, e->r_zs), e->r_zs.n, nxt, e->max_ch, s), "z-solve");
+    for (int q = 0; q < kZsChunks; ++q)
+        ENS_CK(launch_zsolve_ens(I, items_at(e, e->r_zs[q]), e->r_zs[q].n, nxt, kZsChunkValues[q], s),
+               "z-solve");
     ENS_CK(launch_div_pack_ens(I, items_at(e, e->r_div), e->r_div.n, nxt, s), "divergence");
     for (auto &gr : e->groups) {
         ENS_FFT(cufftSetStream(gr.fwd, s), "cufftSetStream");
@@ -428,7 +433,6 @@ int slc_ensemble_bind(slc_ensemble *e, double *const *lev, double *const *p, con
         }
         gr.plans = true;
     }
-    e->max_ch = 1;
     for (int i = 0; i < n; ++i) {
         slc_grid *g = e->grids[i];
         const SlcParams &P = g->P;
@@ -467,7 +471,6 @@ int slc_ensemble_bind(slc_ensemble *e, double *const *lev, double *const *p, con
         e->zs_tabs[i] = tab;
         I.zs_uv = tab;
         I.zs_w = tab + half;
-        e->max_ch = std::max(e->max_ch, zsolve_chunk(P.nz));
         I.partials = g->partials;
         I.scal = g->scal;
         I.ncl = nclamp ? (unsigned long long *)(nclamp + i) : e->d_ncl + i;

@@ -143,9 +143,12 @@ int sl_mixed_ens_blocks_per_sm();  // resident blocks of the mixed persistent ke
 // U* for every instance: items (inst, comp, chunk of 1024 elements).
 cudaError_t launch_lincomb_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph,
                                cudaStream_t s);
-// zsolve.cu: items (inst, block of kZWarps columns); chunk sizes up to max_ch.
+// zsolve.cu: items (inst, block of kZWarps columns) of instances whose
+// zsolve_chunk(nz) is ch.
+constexpr int kZsChunks = 7;
+constexpr int kZsChunkValues[kZsChunks] = {1, 2, 4, 8, 12, 16, 32};
 cudaError_t launch_zsolve_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
-                              int max_ch, cudaStream_t s);
+                              int ch, cudaStream_t s);
 int zsolve_ens_warps();
 // poisson.cu
 cudaError_t launch_bc_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,

@@ -192,29 +192,22 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zsolve(SlcParams P, double *u,
                     zsm + wib * zpad(32 * CH));
 }
 
-// Ensemble form: item (inst, block index); the instance's chunk size picks
-// the instantiation, so each channel is solved exactly as on its own.
+// Ensemble form: item (inst, block index) over the instances whose chunk
+// size is CH (the caller groups them), so each channel is solved exactly as
+// on its own, and each launch carries one instantiation's registers and
+// shared memory rather than the largest one's.
+template <int CH>
 __global__ void __launch_bounds__(kZWarps * 32) k_zsolve_ens(const EnsInst *__restrict__ ins,
                                                              const EnsItem *__restrict__ items,
-                                                             int lvl, int max_ch)
+                                                             int lvl)
 {
     extern __shared__ double zsm[];
     const EnsItem it = items[blockIdx.x];
     const EnsInst &I = ins[it.inst];
-    const SlcParams &P = I.P;
     const int wib = threadIdx.x >> 5;
     const long long wid = (long long)it.a * kZWarps + wib;
-    double *sm = zsm + wib * zpad(32 * max_ch);
-    double *u = I.lev[lvl][0], *v = I.lev[lvl][1], *w = I.lev[lvl][2];
-    switch (zsolve_chunk(P.nz)) {
-    case 1: zsolve_warp<1>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
-    case 2: zsolve_warp<2>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
-    case 4: zsolve_warp<4>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
-    case 8: zsolve_warp<8>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
-    case 12: zsolve_warp<12>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
-    case 16: zsolve_warp<16>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
-    default: zsolve_warp<32>(P, u, v, w, I.zs_uv, I.zs_w, wid, sm); break;
-    }
+    zsolve_warp<CH>(I.P, I.lev[lvl][0], I.lev[lvl][1], I.lev[lvl][2], I.zs_uv, I.zs_w, wid,
+                    zsm + wib * zpad(32 * CH));
 }
 
 }  // namespace
@@ -325,17 +318,34 @@ extern "C" int slc_zsolve_noalloc(int nx, int ny, int nz, double nu, int top_wal
 
 int zsolve_ens_warps() { return kZWarps; }
 
-cudaError_t launch_zsolve_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
-                              int max_ch, cudaStream_t s)
+namespace {
+template <int CH>
+cudaError_t launch_zsolve_ens_ch(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                                 cudaStream_t s)
 {
-    if (nitems <= 0) return cudaSuccess;
-    const size_t smem = (size_t)kZWarps * zpad(32 * max_ch) * sizeof(double);
+    const size_t smem = (size_t)kZWarps * zpad(32 * CH) * sizeof(double);
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_zsolve_ens, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_zsolve_ens<CH>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    k_zsolve_ens<<<nitems, kZWarps * 32, smem, s>>>(ins, items, lvl, max_ch);
+    k_zsolve_ens<CH><<<nitems, kZWarps * 32, smem, s>>>(ins, items, lvl);
     count_launches(1);
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_zsolve_ens(const EnsInst *ins, const EnsItem *items, int nitems, int lvl,
+                              int ch, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    switch (ch) {
+    case 1: return launch_zsolve_ens_ch<1>(ins, items, nitems, lvl, s);
+    case 2: return launch_zsolve_ens_ch<2>(ins, items, nitems, lvl, s);
+    case 4: return launch_zsolve_ens_ch<4>(ins, items, nitems, lvl, s);
+    case 8: return launch_zsolve_ens_ch<8>(ins, items, nitems, lvl, s);
+    case 12: return launch_zsolve_ens_ch<12>(ins, items, nitems, lvl, s);
+    case 16: return launch_zsolve_ens_ch<16>(ins, items, nitems, lvl, s);
+    default: return launch_zsolve_ens_ch<32>(ins, items, nitems, lvl, s);
+    }
 }
