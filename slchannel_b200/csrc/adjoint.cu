@@ -600,9 +600,33 @@ __global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double *_
     *dst += acc;
 }
 
-__global__ void __launch_bounds__(kT) k_pull_tri(SlcParams P, int c, const double4 *__restrict__ pay,
-                                                 const int *__restrict__ order,
-                                                 const int *__restrict__ starts, double *lam)
+// Trilinear transposes in two passes.  About 9 records share each base key
+// (every arrival point's trajectory samples land in each field's grid), so
+// (1) one thread per key sums its records into the 8 corner partials of that
+// base, records in sorted order, stored corner-major S[corner * nkeys + key];
+// (2) each node adds the partials of the 8 bases covering it, corners in a
+// fixed order.  Both orders are fixed, so the result is reproducible.
+__global__ void __launch_bounds__(kT) k_tri_segsum(const double4 *__restrict__ pay,
+                                                   const int *__restrict__ order,
+                                                   const int *__restrict__ starts, long long nkeys,
+                                                   double *__restrict__ S)
+{
+    const long long key = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (key >= nkeys) return;
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int a = __ldg(starts + key), b = __ldg(starts + key + 1);
+    for (int p = a; p < b; ++p) {
+        const double4 R = pay[__ldg(order + p)];
+        const double wx[2] = {1.0 - R.x, R.x}, wy[2] = {1.0 - R.y, R.y}, wz[2] = {1.0 - R.z, R.z};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] = fma(R.w, wx[q >> 2] * wy[(q >> 1) & 1] * wz[q & 1], acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) S[(size_t)q * nkeys + key] = acc[q];
+}
+
+__global__ void __launch_bounds__(kT) k_pull_tri(SlcParams P, int c, const double *__restrict__ S,
+                                                 double *lam)
 {
     const int NZ = c < 2 ? P.nz + 2 : P.nz + 1;
     const int kmax = c < 2 ? P.nz : P.nz - 1;  // largest base interval
@@ -613,21 +637,18 @@ __global__ void __launch_bounds__(kT) k_pull_tri(SlcParams P, int c, const doubl
     const int iy = (int)((t / NZ) % P.ny);
     const int ix = (int)(t / ((long long)NZ * P.ny));
     double acc = 0.0;
+#pragma unroll
     for (int mx = 0; mx < 2; ++mx) {
         const int bx = wrapn(ix - mx, P.nx);
+#pragma unroll
         for (int my = 0; my < 2; ++my) {
             const int by = wrapn(iy - my, P.ny);
+#pragma unroll
             for (int mz = 0; mz < 2; ++mz) {
                 const int k0 = iz - mz;
                 if (k0 < 0 || k0 > kmax) continue;
-                const int key = (bx * P.ny + by) * NZ + k0;
-                const int a = __ldg(starts + key), b = __ldg(starts + key + 1);
-                for (int p = a; p < b; ++p) {
-                    const double4 R = pay[__ldg(order + p)];
-                    const double w = (mx ? R.x : 1.0 - R.x) * (my ? R.y : 1.0 - R.y) *
-                                     (mz ? R.z : 1.0 - R.z);
-                    acc = fma(R.w, w, acc);
-                }
+                const long long key = ((long long)bx * P.ny + by) * NZ + k0;
+                acc += __ldg(S + (size_t)(mx * 4 + my * 2 + mz) * nn + key);
             }
         }
     }
@@ -976,6 +997,7 @@ struct AdjWS {
     double *scratch = nullptr, *partials = nullptr, *S = nullptr;
     double *W = nullptr;  // sorted gather weights, 3 O arrays of n_c[0]
     int *kz = nullptr;    // sorted gather records' first z node
+    double *Stri = nullptr;  // trilinear corner partials, 8 arrays of nkeys_max
 };
 
 namespace {
@@ -1033,6 +1055,7 @@ int ensure_adj(slc_grid *g)
     if (!rc) rc = adj_alloc(g, &w->S, (size_t)1, "adjoint sum");
     if (!rc) rc = adj_alloc(g, &w->W, (size_t)3 * SLC_MAX_ORDER * w->n_c[0], "adjoint gather weights");
     if (!rc) rc = adj_alloc(g, &w->kz, (size_t)w->n_c[0], "adjoint gather z bases");
+    if (!rc) rc = adj_alloc(g, &w->Stri, (size_t)8 * w->nkeys_max, "adjoint trilinear partials");
     if (rc) {
         delete w;
         return rc;
@@ -1124,8 +1147,9 @@ int sl_adjoint_t(slc_grid *g, AdjWS *w, const V3 &M, const double *const cur[3],
         const long long nkeys = (long long)P.nx * P.ny * NZ;
         int rc = sort_records(g, w, nrec, nkeys, s);
         if (rc) return rc;
-        k_pull_tri<<<nblk(nkeys), kT, 0, s>>>(P, c, w->pay, w->order, w->starts, w->lam_mid[c]);
-        count_launches(1);
+        k_tri_segsum<<<nblk(nkeys), kT, 0, s>>>(w->pay, w->order, w->starts, nkeys, w->Stri);
+        k_pull_tri<<<nblk(nkeys), kT, 0, s>>>(P, c, w->Stri, w->lam_mid[c]);
+        count_launches(2);
         // U* = 2 V^n - V^{n-1} (BDF2) or V^n (BDF1)
         const long long ne = (long long)g->ghost_elems[c];
         k_axpy<<<148 * 8, kT, 0, s>>>(lam_cur[c], w->lam_mid[c], MODE == 2 ? 2.0 : 1.0, ne);
