@@ -564,8 +564,8 @@ def measure_adjoint(n_dirs):
            "forward_ms": ms_fwd, "gradient_ms": ms_grad,
            "adjoint_ms_per_step": (ms_grad - ms_fwd) / steps,
            "backward_over_forward": (ms_grad - ms_fwd) / ms_fwd,
-           "fd_directions": n_dirs, "fd_h": 1e-6, "fd_max_rel_err": worst,
-           "fd_median_rel_err": sorted(errs)[len(errs) // 2],
+           "fd_directions": n_dirs, "fd_h": 1e-6, "fd_max_rel_err": worst if errs else None,
+           "fd_median_rel_err": sorted(errs)[len(errs) // 2] if errs else None,
            "workload": "128x96x128, 2pi x pi x 2, Re_b 2800, dt 0.01, order 6, FP64, 50 steps, "
                        "checkpoints every 10, loss = masked kinetic energy of V^50"}
     del flow, V0, grad
