@@ -564,6 +564,10 @@ __global__ void k_sort_segments(const int *__restrict__ starts, long long nkeys,
 // coalesced loads per record (lanes are consecutive iz, their ranges shifted
 // by one key).  Records are summed in key order, then record id: a fixed
 // order, so the result is reproducible bit for bit.
+#ifndef SLC_PULL_UNROLL
+#define SLC_PULL_UNROLL 2
+#endif
+constexpr int kPullUnroll = SLC_PULL_UNROLL;  // records per trip of the pull's inner loop
 template <int C, int O>
 __global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double *__restrict__ W,
                                                     const int *__restrict__ kz, long long nrec,
@@ -587,6 +591,7 @@ __global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double *_
                 const double *wyv = W + (size_t)(O + my) * nrec;
                 const int kb = (bx * P.ny + by) * NZ;
                 const int a = __ldg(starts + kb + klo), b = __ldg(starts + kb + khi + 1);
+#pragma unroll kPullUnroll
                 for (int p = a; p < b; ++p) {
                     const int mz = iz - __ldg(kz + p);
                     const double wz = __ldg(W + (size_t)(2 * O + mz) * nrec + p);
