@@ -45,6 +45,18 @@ __device__ __forceinline__ int wrapn(int i, int n)
     return i < 0 ? i + n : i;
 }
 
+// Periodic wrap of i in (-6, n + 6) (a stencil base plus an offset below 6):
+// branch-free for n >= 6 (n is uniform, so no divergence), modulo otherwise.
+__device__ __forceinline__ int wrap6(int i, int n)
+{
+    if (n >= 6) {
+        i += (i < 0) ? n : 0;
+        i -= (i >= n) ? n : 0;
+        return i;
+    }
+    return wrapn(i, n);
+}
+
 struct V3 {
     NodeView<double> u, v, w;
 };
@@ -148,10 +160,10 @@ __device__ void grad_interp(const SlcParams &P, NodeView<double> F, double x, do
     zbasis_all<O>(zn, dinv, denom_rows(Comp<C>::centers, P.nz, O), b.k0, z, wz, dwz);
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (int i = 0; i < O; ++i) {
-        const int xo = wrapn(b.bx0 + i, P.nx) * F.sx;
+        const int xo = wrap6(b.bx0 + i, P.nx) * F.sx;
         double sy_w = 0.0, sy_dw = 0.0, sy_wz = 0.0;
         for (int j = 0; j < O; ++j) {
-            const double *row = F.p + xo + wrapn(b.by0 + j, P.ny) * F.sy + b.k0;
+            const double *row = F.p + xo + wrap6(b.by0 + j, P.ny) * F.sy + b.k0;
             double s = 0.0, sd = 0.0;
 #pragma unroll
             for (int k = 0; k < O; ++k) {
@@ -584,10 +596,10 @@ __global__ void __launch_bounds__(kT) k_pull_gather(SlcParams P, const double *_
     double acc = 0.0;
     if (klo <= khi) {
         for (int mx = 0; mx < O; ++mx) {
-            const int bx = wrapn(ix - mx, P.nx);
+            const int bx = wrap6(ix - mx, P.nx);
             const double *cwx = W + (size_t)mx * nrec;
             for (int my = 0; my < O; ++my) {
-                const int by = wrapn(iy - my, P.ny);
+                const int by = wrap6(iy - my, P.ny);
                 const double *wyv = W + (size_t)(O + my) * nrec;
                 const int kb = (bx * P.ny + by) * NZ;
                 const int a = __ldg(starts + kb + klo), b = __ldg(starts + kb + khi + 1);
@@ -644,10 +656,10 @@ __global__ void __launch_bounds__(kT) k_pull_tri(SlcParams P, int c, const doubl
     double acc = 0.0;
 #pragma unroll
     for (int mx = 0; mx < 2; ++mx) {
-        const int bx = wrapn(ix - mx, P.nx);
+        const int bx = wrap6(ix - mx, P.nx);
 #pragma unroll
         for (int my = 0; my < 2; ++my) {
-            const int by = wrapn(iy - my, P.ny);
+            const int by = wrap6(iy - my, P.ny);
 #pragma unroll
             for (int mz = 0; mz < 2; ++mz) {
                 const int k0 = iz - mz;
@@ -677,7 +689,7 @@ __global__ void k_diff_adj(SlcParams P, const double *__restrict__ lh, double *l
     const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
     const size_t sx = (size_t)g.Y * g.Z, sy = g.Z;
     auto at = [&](int ii, int jj) {
-        return lh[(size_t)(wrapn(ii, P.nx) + 1) * sx + (size_t)(wrapn(jj, P.ny) + 1) * sy + (k + 1)];
+        return lh[(size_t)(wrap6(ii, P.nx) + 1) * sx + (size_t)(wrap6(jj, P.ny) + 1) * sy + (k + 1)];
     };
     const double c0 = at(i, j);
     const double lap = (at(i + 1, j) - 2.0 * c0 + at(i - 1, j)) * P.inv_dx2 +
