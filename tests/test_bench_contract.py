@@ -66,3 +66,30 @@ def test_reference_arm_torchrun_rank0_only():
     assert len(lines) == 1
     d = lines[0]
     assert d["impl"] == "reference" and d["value"] > 0
+
+
+@pytest.mark.gpu
+def test_gpu_arm_json_line():
+    r = _run([sys.executable, "bench.py", "--n", "64", "--steps", "3", "--warmup", "3",
+              "--e2e-steps", "2", "--mixed-error-steps", "2", "--no-ensemble", "--no-adjoint",
+              "--no-schemes"])
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1
+    d = lines[0]
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+              "roofline", "cpu_baseline", "e2e", "gpu_launches", "clocks"):
+        assert k in d, k
+    assert d["value"] > 0 and d["steps"] == 3 and d["warmup"] == 3 and d["n_gpus"] == 1
+    assert abs(d["ms_per_step"] * d["value"] - 1000.0) < 1e-6 * 1000.0
+    rl = d["roofline"]
+    assert rl["bound"] in ("hbm", "tensor") and rl["unit"] in ("GB/s", "TFLOP/s")
+    assert rl["achieved"] > 0 and rl["peak"] > 0 and abs(rl["frac"] - rl["achieved"] / rl["peak"]) < 1e-12
+    assert rl["fp64_pipe"]["peak"] > 0 and 0 < rl["fp64_pipe"]["frac"]
+    cb = d["cpu_baseline"]
+    assert cb["value"] > 0 and cb["cores"] >= 1 and cb["kind"] in ("port", "reference")
+    e = d["e2e"]
+    assert e["value"] > 0 and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
+    assert d["gpu_launches"] > 0
+    assert d["mixed"]["value"] > 0 and d["mixed"]["rel_linf_err_vs_fp64"] < 1e-4
