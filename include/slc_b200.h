@@ -55,7 +55,7 @@ typedef struct {
     double gamma;              /* tanh stretching parameter */
     int32_t stretching;        /* 0 = 'symmetric', 1 = 'bottom' */
     int32_t order;             /* 4 (tricubic) or 6 (triquintic) */
-    int32_t traj_order;        /* 2 (trilinear) or 4 (tricubic Lagrange; FP64 precision only) */
+    int32_t traj_order;        /* 2 (trilinear) or 4 (tricubic Lagrange) */
     int32_t n_traj_iters;      /* midpoint fixed-point iterations (>= 1) */
     int32_t top_wall_neumann;  /* 0 = 'dirichlet' (no-slip), 1 = 'neumann' */
     int32_t precision;         /* SLC_PREC_FP64 or SLC_PREC_MIXED */

@@ -23,6 +23,7 @@
 struct slc_ensemble {
     int device = 0;
     int order = 6;
+    int traj = 2;  // the instances' common trajectory order, 0 when they differ
     int mixed = 0;  // all instances in the mixed form
     std::vector<slc_grid *> grids;
     std::vector<EnsInst> host_inst;
@@ -271,7 +272,7 @@ int enqueue_step(slc_ensemble *e, int ph, cudaStream_t s)
         ENS_CK(cudaMemsetAsync(e->host_inst[i].ncl, 0, sizeof(unsigned long long), s), "memset");
     ENS_CK(cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned), s), "memset");
     if (e->mixed)
-        ENS_CK(launch_sl_mixed_ens(I, items_at(e, e->r_sl), e->r_sl.n, ph, e->order, e->d_queue,
+        ENS_CK(launch_sl_mixed_ens(I, items_at(e, e->r_sl), e->r_sl.n, ph, e->order, e->traj, e->d_queue,
                                    e->sl_grid, s),
                "mixed trace+gather BDF2");
     else
@@ -326,6 +327,9 @@ int slc_ensemble_create(const slc_grid_desc *descs, int n, slc_ensemble **out)
     slc_ensemble *e = new slc_ensemble();
     e->device = descs[0].device;
     e->order = descs[0].order;
+    e->traj = descs[0].traj_order;
+    for (int i = 1; i < n; ++i)
+        if (descs[i].traj_order != e->traj) e->traj = 0;  // a mixture: read per instance
     e->mixed = descs[0].precision == SLC_PREC_MIXED ? 1 : 0;
     DevGuard dg(e->device);
     for (int i = 0; i < n; ++i) {
@@ -601,7 +605,7 @@ int slc_ensemble_autotune(slc_ensemble *e, int phase, int reps, int *tkl_out, do
                 if (ce == cudaSuccess && r == 1) ce = cudaEventRecord(a, s);
                 if (ce == cudaSuccess)
                     ce = e->mixed ? launch_sl_mixed_ens(e->d_inst, d_tmp, (int)items.size(), phase, e->order,
-                                                        e->d_queue, e->sl_grid, s)
+                                                        e->traj, e->d_queue, e->sl_grid, s)
                                   : launch_sl_ens(e->d_inst, d_tmp, (int)items.size(), phase, e->order,
                                                   e->d_queue, e->sl_grid, s);
             }

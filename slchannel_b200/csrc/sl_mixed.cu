@@ -163,8 +163,15 @@ __device__ __forceinline__ void sample3_32(const SlcParams &P, const Vel3M &M, c
     ws = tri32(M.w, ib0, ib1, txb, jb0, jb1, tyb, kf, wf0, wf1);
 }
 
+// Tricubic trajectory velocity (traj_interp_order 4), defined below.
+__device__ __noinline__ void sample3_32_o4(const SlcParams &P, const Vel3M &M, const Arr32 &A,
+                                           float ddx, float ddy, float dz, float &us, float &vs,
+                                           float &ws);
+
 // Iterated midpoint rule (semilag.py:542-552) in FP32 displacements; returns
 // the foot as displacements from the arrival point (x, y in index units).
+// TO: trajectory sampling order 2 or 4, or 0 to read P.traj_order.
+template <int TO>
 __device__ __forceinline__ void trace_foot32(const SlcParams &P, const Vel3M &M, const Arr32 &A,
                                              float hdt, float us0, float vs0, float ws0,
                                              float &ddx, float &ddy, float &ddz)
@@ -175,7 +182,8 @@ __device__ __forceinline__ void trace_foot32(const SlcParams &P, const Vel3M &M,
     float mz = clampdz(A, -hdt * ws0);
     for (int it = 1; it < P.n_iters; ++it) {
         float us, vs, ws;
-        sample3_32(P, M, A, mx, my, mz, us, vs, ws);
+        if (TO == 4 || (TO == 0 && P.traj_order == 4)) sample3_32_o4(P, M, A, mx, my, mz, us, vs, ws);
+        else sample3_32(P, M, A, mx, my, mz, us, vs, ws);
         mx = -hdt * us * idx;
         my = -hdt * vs * idy;
         mz = clampdz(A, -hdt * ws);
@@ -187,8 +195,9 @@ __device__ __forceinline__ void trace_foot32(const SlcParams &P, const Vel3M &M,
 
 // Clamp-and-count the foot and interpolate the mixed field F there: FP32
 // weights and accumulation for the fluctuation, the FP64 mean profile through
-// the (FP32) z weights.
-template <int C, int O>
+// the (FP32) z weights.  MEAN32: the mean profile rounded to FP32 and summed
+// in FP32 instead, as the trajectory samples do.
+template <int C, int O, bool MEAN32 = false>
 __device__ __forceinline__ double gather_foot32(const SlcParams &P, MixedView F, const Arr32 &A,
                                                 float ddx, float ddy, float ddz, unsigned &ncl)
 {
@@ -248,10 +257,32 @@ __device__ __forceinline__ double gather_foot32(const SlcParams &P, MixedView F,
         }
         acc = fmaf(st.wx[i], accy, acc);
     }
+    if constexpr (MEAN32) {
+        float m = 0.f;
+#pragma unroll
+        for (int k = 0; k < O; ++k) m = fmaf(st.wz[k], __ldg(F.mean32 + k0 + k), m);
+        return (double)(acc + m);
+    }
     double mean = 0.0;
 #pragma unroll
     for (int k = 0; k < O; ++k) mean = fma((double)st.wz[k], __ldg(F.mean + k0 + k), mean);
     return (double)acc + mean;
+}
+
+// The trajectory velocity with tricubic Lagrange sampling (traj_interp_order
+// 4, semilag.py:206-209, 512-528): the order-4 mixed gather of each U*
+// component at arrival + displacement, on that component's own node grid
+// (gather_foot32 picks the grid's shifts from the arrival record), all in
+// FP32 like the trilinear samples (FP32 mean profile).  The midpoint is
+// already inside [z_lo, z_hi]; no clamp is counted.
+__device__ __noinline__ void sample3_32_o4(const SlcParams &P, const Vel3M &M, const Arr32 &A,
+                                           float ddx, float ddy, float dz, float &us, float &vs,
+                                           float &ws)
+{
+    unsigned none = 0;
+    us = (float)gather_foot32<0, 4, true>(P, M.u, A, ddx, ddy, dz, none);
+    vs = (float)gather_foot32<1, 4, true>(P, M.v, A, ddx, ddy, dz, none);
+    ws = (float)gather_foot32<2, 4, true>(P, M.w, A, ddx, ddy, dz, none);
 }
 
 struct NodeValMixed32 {
@@ -282,7 +313,7 @@ __device__ __forceinline__ double xy_diffusion64(const SlcParams &P, const doubl
 // MODE 0: one foot of A (advect); 1: BDF1 predictor; 2: BDF2 predictor.
 // FA/FB: the mixed views of the near (V^n) and far (V^{n-1}) fields of
 // component C; fn/fnm1: the same fields in FP64 (ghost-shaped) for R.
-template <int C, int O, int MODE>
+template <int C, int O, int MODE, int TO = 0>
 __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &M, const MixedView &FA,
                                                const MixedView &FB, const double *__restrict__ fn,
                                                const double *__restrict__ fnm1, double dt,
@@ -292,11 +323,20 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
     const int nzi = (C == 2) ? P.nz - 1 : P.nz;
     if (k < nzi && j < P.ny) {
         const Arr32 A = arrival32<C>(P, i, j, k);
-        double u0, v0, w0;
-        arrival_sample<C>(P, M, i, j, k, NodeValMixed32(), u0, v0, w0);
-        const float us0 = (float)u0, vs0 = (float)v0, ws0 = (float)w0;
+        // first fixed-point sample at the arrival point: exact node values
+        // for trilinear sampling, the tricubic stencils otherwise
+        float us0, vs0, ws0;
+        if (TO == 4 || (TO == 0 && P.traj_order == 4)) {
+            sample3_32_o4(P, M, A, 0.f, 0.f, 0.f, us0, vs0, ws0);
+        } else {
+            double u0, v0, w0;
+            arrival_sample<C>(P, M, i, j, k, NodeValMixed32(), u0, v0, w0);
+            us0 = (float)u0;
+            vs0 = (float)v0;
+            ws0 = (float)w0;
+        }
         float ddx, ddy, ddz;
-        trace_foot32(P, M, A, (float)(0.5 * dt), us0, vs0, ws0, ddx, ddy, ddz);
+        trace_foot32<TO>(P, M, A, (float)(0.5 * dt), us0, vs0, ws0, ddx, ddy, ddz);
         const double ubar = gather_foot32<C, O>(P, FA, A, ddx, ddy, ddz, ncl);
         double res;
         if (MODE == 0) {
@@ -304,7 +344,7 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
         } else if (MODE == 1) {
             res = ubar + dt * xy_diffusion64<C>(P, fn, i, j, k);
         } else {
-            trace_foot32(P, M, A, (float)dt, us0, vs0, ws0, ddx, ddy, ddz);
+            trace_foot32<TO>(P, M, A, (float)dt, us0, vs0, ws0, ddx, ddy, ddz);
             const double ubb = gather_foot32<C, O>(P, FB, A, ddx, ddy, ddz, ncl);
             const double Rn = xy_diffusion64<C>(P, fn, i, j, k);
             const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion64<C>(P, fnm1, i, j, k);
@@ -316,7 +356,7 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
     }
 }
 
-template <int C, int O, int MODE>
+template <int C, int O, int MODE, int TO>
 __global__ void __launch_bounds__(kThreads, SLC_SLM_MIN_BLOCKS)
     k_sl_mixed(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3M M,
                const __grid_constant__ MixedView FA, const __grid_constant__ MixedView FB,
@@ -328,7 +368,7 @@ __global__ void __launch_bounds__(kThreads, SLC_SLM_MIN_BLOCKS)
     const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
     const int i = blockIdx.z;
     unsigned ncl = 0;
-    sl_point_mixed<C, O, MODE>(P, M, FA, FB, fn, fnm1, dt, out, i, j, k, ncl);
+    sl_point_mixed<C, O, MODE, TO>(P, M, FA, FB, fn, fnm1, dt, out, i, j, k, ncl);
     add_clamps(nclamp, ncl);
 }
 
@@ -575,7 +615,9 @@ __global__ void __launch_bounds__(1024) k_pack_mixed_ens(const EnsInst *__restri
 
 // Persistent mixed-form BDF2 trace+gather over the (instance, component, x
 // index, tile) queue; the structure of the FP64 ensemble kernel.
-template <int O>
+// TO: the instances' common trajectory order (2 or 4), or 0 for a mixture
+// (read per instance).
+template <int O, int TO>
 __global__ void __launch_bounds__(kThreads, SLC_SLM_ENS_MIN_BLOCKS) k_sl_mixed_ens(const EnsInst *__restrict__ ins,
                                                               const EnsItem *__restrict__ items,
                                                               int nitems, int ph, unsigned *queue)
@@ -608,9 +650,9 @@ __global__ void __launch_bounds__(kThreads, SLC_SLM_ENS_MIN_BLOCKS) k_sl_mixed_e
         const double *fnm1 = I.lev[ens_prev(ph)][w.a];
         double *out = I.lev[ens_next(ph)][w.a];
         unsigned ncl = 0;
-        if (w.a == 0) sl_point_mixed<0, O, 2>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
-        else if (w.a == 1) sl_point_mixed<1, O, 2>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
-        else sl_point_mixed<2, O, 2>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
+        if (w.a == 0) sl_point_mixed<0, O, 2, TO>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else if (w.a == 1) sl_point_mixed<1, O, 2, TO>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else sl_point_mixed<2, O, 2, TO>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
         add_clamps(I.ncl, ncl);
     }
 }
@@ -625,21 +667,29 @@ MixedView mview(const MixedWS &ws, int slot, const SlcParams &P)
     return v;
 }
 
-template <int O, int MODE>
-void launch_t(const SlcParams &P, Tri fn, Tri fnm1, const MixedWS &ws, double dt, TriMut out,
-              unsigned long long *ncl, cudaStream_t s)
+template <int O, int MODE, int TO>
+void launch_tt(const SlcParams &P, Tri fn, Tri fnm1, const MixedWS &ws, double dt, TriMut out,
+               unsigned long long *ncl, cudaStream_t s)
 {
     Vel3M M{mview(ws, 6, P), mview(ws, 7, P), mview(ws, 8, P)};
     const dim3 gc((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
     const dim3 gw((P.nz - 1 + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
-    k_sl_mixed<0, O, MODE><<<gc, kThreads, 0, s>>>(P, M, mview(ws, 0, P), mview(ws, 3, P), fn.u,
+    k_sl_mixed<0, O, MODE, TO><<<gc, kThreads, 0, s>>>(P, M, mview(ws, 0, P), mview(ws, 3, P), fn.u,
                                                     fnm1.u, dt, out.u, ncl);
-    k_sl_mixed<1, O, MODE><<<gc, kThreads, 0, s>>>(P, M, mview(ws, 1, P), mview(ws, 4, P), fn.v,
+    k_sl_mixed<1, O, MODE, TO><<<gc, kThreads, 0, s>>>(P, M, mview(ws, 1, P), mview(ws, 4, P), fn.v,
                                                     fnm1.v, dt, out.v, ncl);
     if (P.nz > 1)
-        k_sl_mixed<2, O, MODE><<<gw, kThreads, 0, s>>>(P, M, mview(ws, 2, P), mview(ws, 5, P),
+        k_sl_mixed<2, O, MODE, TO><<<gw, kThreads, 0, s>>>(P, M, mview(ws, 2, P), mview(ws, 5, P),
                                                         fn.w, fnm1.w, dt, out.w, ncl);
     count_launches(P.nz > 1 ? 3 : 2);
+}
+
+template <int O, int MODE>
+void launch_t(const SlcParams &P, Tri fn, Tri fnm1, const MixedWS &ws, double dt, TriMut out,
+              unsigned long long *ncl, cudaStream_t s)
+{
+    if (P.traj_order == 4) launch_tt<O, MODE, 4>(P, fn, fnm1, ws, dt, out, ncl, s);
+    else launch_tt<O, MODE, 2>(P, fn, fnm1, ws, dt, out, ncl, s);
 }
 
 }  // namespace
@@ -705,11 +755,16 @@ int mixed_mean_blocks() { return kMeanBlocks; }
 
 int sl_mixed_ens_blocks_per_sm()
 {
-    int nb = 0, nb4 = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sl_mixed_ens<6>, kThreads, 0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb4, k_sl_mixed_ens<4>, kThreads, 0) != cudaSuccess)
-        return 1;
-    const int m = nb < nb4 ? nb : nb4;
+    // the smallest residency over the instantiations the ensemble may launch
+    const void *k[6] = {(const void *)k_sl_mixed_ens<6, 2>, (const void *)k_sl_mixed_ens<4, 2>,
+                        (const void *)k_sl_mixed_ens<6, 4>, (const void *)k_sl_mixed_ens<4, 4>,
+                        (const void *)k_sl_mixed_ens<6, 0>, (const void *)k_sl_mixed_ens<4, 0>};
+    int m = 1 << 30;
+    for (int q = 0; q < 6; ++q) {
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k[q], kThreads, 0) != cudaSuccess) return 1;
+        m = nb < m ? nb : m;
+    }
     return m > 0 ? m : 1;
 }
 int mixed_pack_cols() { return kPackJ; }
@@ -728,11 +783,21 @@ cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsIte
 }
 
 cudaError_t launch_sl_mixed_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
+                                int traj,
                                 unsigned *queue, int grid, cudaStream_t s)
 {
     if (nitems <= 0) return cudaSuccess;
-    if (order == 4) k_sl_mixed_ens<4><<<grid, kThreads, 0, s>>>(ins, items, nitems, ph, queue);
-    else k_sl_mixed_ens<6><<<grid, kThreads, 0, s>>>(ins, items, nitems, ph, queue);
+#define SLM_ENS(OV, TV) k_sl_mixed_ens<OV, TV><<<grid, kThreads, 0, s>>>(ins, items, nitems, ph, queue)
+    if (order == 4) {
+        if (traj == 2) SLM_ENS(4, 2);
+        else if (traj == 4) SLM_ENS(4, 4);
+        else SLM_ENS(4, 0);
+    } else {
+        if (traj == 2) SLM_ENS(6, 2);
+        else if (traj == 4) SLM_ENS(6, 4);
+        else SLM_ENS(6, 0);
+    }
+#undef SLM_ENS
     count_launches(1);
     return cudaGetLastError();
 }

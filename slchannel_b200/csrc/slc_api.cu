@@ -337,8 +337,6 @@ int slc_grid_create(const slc_grid_desc *d, slc_grid **out)
         return fail(nullptr, SLC_E_INVALID, "sl.interp_order must be 4 (tricubic) or 6 (triquintic), got " + std::to_string(d->order));
     if (d->traj_order != 2 && d->traj_order != 4)
         return fail(nullptr, SLC_E_INVALID, "sl.traj_interp_order must be 2 (trilinear) or 4 (tricubic), got " + std::to_string(d->traj_order));
-    if (d->traj_order == 4 && d->precision == SLC_PREC_MIXED)
-        return fail(nullptr, SLC_E_INVALID, "the mixed form samples the trajectory trilinearly (traj_interp_order 2)");
     if (d->n_traj_iters < 1)
         return fail(nullptr, SLC_E_INVALID, "sl.n_traj_iters must be >= 1");
     if (d->stretching != 0 && d->stretching != 1)

@@ -195,5 +195,7 @@ int mixed_pack_threads(int nzp);     // its block size for nzp padded levels
 cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsItem *pp_items, int n_pp,
                                      const EnsItem *pack_items, int n_pack, int pack_threads, int ph,
                                      cudaStream_t s);
+// traj: the instances' common trajectory order (2 or 4), 0 when they differ
 cudaError_t launch_sl_mixed_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
+                                int traj,
                                 unsigned *queue, int grid, cudaStream_t s);

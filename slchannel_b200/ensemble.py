@@ -66,7 +66,8 @@ def _config(spec, order, precision):
         "initialization": {"type": "parabolic"},
         "time": {"dt": 0.01, "dt_update_interval": 0},
         "compute": {"device": "cuda"},
-        "sl": {"interp_order": order, "n_traj_iters": 2, "interp_dtype": precision},
+        "sl": {"interp_order": order, "n_traj_iters": 2, "interp_dtype": precision,
+               "traj_interp_order": spec.get("traj_order", 2)},
     }
 
 

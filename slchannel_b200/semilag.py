@@ -79,9 +79,6 @@ class SLAdvector:
                 f"sl.interp_dtype must be 'fp64', 'fp32_accum64' or 'mixed', got {interp_dtype}")
         if nz + 1 < order:
             raise ValueError(f"nz={nz} too small for interpolation order {order}")
-        if traj_order != 2 and interp_dtype != "fp64":
-            raise NotImplementedError(
-                "the mixed form samples the trajectory trilinearly (traj_interp_order: 2)")
         device = torch.device(device)
         if device.type != "cuda":
             raise RuntimeError("slchannel_b200 runs on a CUDA device (sm_100a); there is no CPU path")

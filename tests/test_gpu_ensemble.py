@@ -72,6 +72,27 @@ def test_ensemble_matches_single_channel_loop(use_graph, precision):
     print(f"ensemble vs loop ({precision}): max relative difference {worst:.3e}")
 
 
+@pytest.mark.parametrize("trajs", [(4, 4, 4, 4, 4), (2, 4, 2, 4, 2)])
+def test_ensemble_mixed_tricubic_trajectories(trajs):
+    """The mixed form with tricubic trajectory sampling: every instance at
+    traj_interp_order 4 (one instantiation), and a mixture of 2 and 4 (read
+    per instance), against the loop over the same single-channel solvers."""
+    specs = [dict(s, traj_order=t) for s, t in zip(_specs(), trajs)]
+    ref, dts = _bootstrapped(specs, "mixed")
+    mine, _ = _bootstrapped(specs, "mixed")
+    ens = ChannelEnsemble(mine, dts, use_graph=True, autotune=False)
+    worst = 0.0
+    for step in range(3):
+        loop_step(ref, dts)
+        ens.step()
+        torch.cuda.synchronize()
+        for i, f in enumerate(ref):
+            for c, a, b in zip("uvw", ens.velocity(i), (f.u, f.v, f.w)):
+                worst = max(worst, _rel(a, b))
+    print(f"tricubic mixed ensemble vs loop {trajs}: max relative difference {worst:.3e}")
+    assert worst <= 1e-13
+
+
 def test_ensemble_tiles_do_not_change_results():
     specs = _specs()
     a_flows, dts = _bootstrapped(specs)

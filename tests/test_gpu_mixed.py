@@ -7,6 +7,9 @@ trace and gather; everything else FP64) against the FP64 oracle.
 * test_mixed_step_error: every SL-BDF2 step, started from the oracle's
   state, within 1e-5 relative velocity error of the FP64 oracle, divergence
   below 1e-11 and the bulk velocity at 1.
+* test_mixed_step_error_traj4: the same with tricubic trajectory sampling
+  (traj_interp_order 4) against the oracle stepping with tricubic
+  trajectories.
 * test_mixed_statistics_drift: free-running 40 steps beside the FP64 GPU
   form; plane-averaged U, u'_rms, v'_rms, w'_rms and uw drift stated and
   bounded."""
@@ -83,6 +86,29 @@ def test_mixed_step_error(order):
     flow = SLChannelFlow(config=_config(n, Lx, Ly, order, "mixed", dt=dt))
     flow.set_state(*(torch.from_numpy(a) for a in (ch.u, ch.v, ch.w, ch.p)))
     for step in range(5):
+        ch.step_bdf2(dt)
+        ub, _ = flow.step_sl_bdf2(dt)
+        for c in "uvw":
+            e = rel_err(getattr(flow, c).cpu().numpy(), getattr(ch, c))
+            assert e < 1e-5, (step, c, e)
+        div = compute_divergence(flow.u, flow.v, flow.w, n, n, n, flow.dx, flow.dy, flow.dz_f)
+        assert div.abs().max().item() < 1e-11
+        assert abs(float(ub) - 1.0) < 1e-12
+        for name in ("u", "v", "w", "u_nm1", "v_nm1", "w_nm1", "p"):
+            getattr(flow, name).copy_(torch.from_numpy(getattr(ch, name)))
+
+
+@pytest.mark.parametrize("order", [6, 4])
+def test_mixed_step_error_traj4(order):
+    n, Lx, Ly, dt, Re = 48, 2 * math.pi, math.pi, 0.02, 2800.0
+    ch0 = _projected(n, Lx, Ly, order, 0.12, 7)
+    ch = OracleChannel(n, n, n, Lx, Ly, 2.0, 2.0, 1.0 / Re, ch0.u, ch0.v, ch0.w, ch0.p,
+                       order=order, traj_order=4, z_f=ch0.z_f, z_c=ch0.z_c)
+    cfg = _config(n, Lx, Ly, order, "mixed", dt=dt)
+    cfg["sl"]["traj_interp_order"] = 4
+    flow = SLChannelFlow(config=cfg)
+    flow.set_state(*(torch.from_numpy(a) for a in (ch.u, ch.v, ch.w, ch.p)))
+    for step in range(4):
         ch.step_bdf2(dt)
         ub, _ = flow.step_sl_bdf2(dt)
         for c in "uvw":
