@@ -10,6 +10,9 @@ trace and gather; everything else FP64) against the FP64 oracle.
 * test_mixed_step_error_traj4: the same with tricubic trajectory sampling
   (traj_interp_order 4) against the oracle stepping with tricubic
   trajectories.
+* test_mixed_inc_pressure: the incremental-pressure form (bdf2_pressure inc),
+  trilinear and tricubic trajectories, free-running 3 steps beside the FP64
+  oracle within 1e-5.
 * test_mixed_statistics_drift: free-running 40 steps beside the FP64 GPU
   form; plane-averaged U, u'_rms, v'_rms, w'_rms and uw drift stated and
   bounded."""
@@ -119,6 +122,28 @@ def test_mixed_step_error_traj4(order):
         assert abs(float(ub) - 1.0) < 1e-12
         for name in ("u", "v", "w", "u_nm1", "v_nm1", "w_nm1", "p"):
             getattr(flow, name).copy_(torch.from_numpy(getattr(ch, name)))
+
+
+@pytest.mark.parametrize("traj", [2, 4])
+def test_mixed_inc_pressure(traj):
+    n, Lx, Ly, dt, Re = 40, 2 * math.pi, math.pi, 0.02, 2800.0
+    ch0 = _projected(n, Lx, Ly, 6, 0.12, 11)
+    ch = OracleChannel(n, n, n, Lx, Ly, 2.0, 2.0, 1.0 / Re, ch0.u, ch0.v, ch0.w, ch0.p, order=6,
+                       traj_order=traj, z_f=ch0.z_f, z_c=ch0.z_c, bdf2_pressure="inc")
+    cfg = _config(n, Lx, Ly, 6, "mixed", dt=dt)
+    cfg["sl"]["traj_interp_order"] = traj
+    cfg["sl"]["bdf2_pressure"] = "inc"
+    flow = SLChannelFlow(config=cfg)
+    flow.set_state(*(torch.from_numpy(a) for a in (ch.u, ch.v, ch.w, ch.p)))
+    for step in range(3):
+        ch.step_bdf2(dt)
+        ub, _ = flow.step_sl_bdf2(dt)
+        for c in "uvw":
+            e = rel_err(getattr(flow, c).cpu().numpy(), getattr(ch, c))
+            assert e < 1e-5, (step, c, e)
+        assert abs(float(ub) - 1.0) < 1e-12
+    div = compute_divergence(flow.u, flow.v, flow.w, n, n, n, flow.dx, flow.dy, flow.dz_f)
+    assert div.abs().max().item() < 1e-11
 
 
 def plane_stats(flow):
