@@ -142,6 +142,9 @@ class ChannelEnsemble:
             raise ValueError("all instances of an ensemble share one precision form")
         if any(f.u_nm1 is None for f in flows):
             raise ValueError("every flow must have taken its BDF1 bootstrap step")
+        if any(f.sl_bdf2_pressure != "noninc" for f in flows):
+            raise ValueError("the ensemble steps the non-incremental pressure form "
+                             "(sl.bdf2_pressure: noninc)")
         L = N.lib()
         self.n = len(flows)
         self.device = flows[0].device

@@ -93,6 +93,15 @@ def test_ensemble_mixed_tricubic_trajectories(trajs):
     assert worst <= 1e-13
 
 
+def test_ensemble_refuses_incremental_pressure():
+    spec = _specs()[0]
+    f, dt = make_flow(spec, order=6)
+    f.sl_bdf2_pressure = "inc"
+    f.step_sl_bdf2(dt)
+    with pytest.raises(ValueError, match="noninc"):
+        ChannelEnsemble([f], [dt], use_graph=False, autotune=False)
+
+
 def test_ensemble_tiles_do_not_change_results():
     specs = _specs()
     a_flows, dts = _bootstrapped(specs)
