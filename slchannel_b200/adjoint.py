@@ -38,6 +38,10 @@ class _Stepper:
     def __init__(self, flow):
         if flow.sl_interp_dtype != "fp64":
             raise ValueError("the adjoint is implemented for the FP64 form")
+        if flow.sl_bdf2_pressure != "noninc" or flow.sl_traj_order != 2:
+            raise ValueError("the adjoint is implemented for the non-incremental pressure form "
+                             "with trilinear trajectories (sl.bdf2_pressure: noninc, "
+                             "sl.traj_interp_order: 2)")
         self.flow = flow
         self.g = flow._grid
         self.p = torch.zeros_like(flow.p)

@@ -23,6 +23,9 @@ def pinned_like(t):
 
 class HostStateStepper:
     def __init__(self, flow):
+        if flow.sl_bdf2_pressure != "noninc":
+            raise ValueError("the host-state step is the non-incremental pressure form "
+                             "(sl.bdf2_pressure: noninc)")
         self.flow = flow
         self._shapes = [tuple(t.shape) for t in (flow.u, flow.v, flow.w, flow.p)]
 

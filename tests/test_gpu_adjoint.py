@@ -123,3 +123,13 @@ def test_adjoint_is_deterministic_and_checkpoint_invariant():
     # ghosts of the returned gradient are zero (folded into the interiors)
     gu = runs[0][0]
     assert float(gu[0].abs().max()) == 0.0 and float(gu[:, 0].abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("attr,value", [("sl_bdf2_pressure", "inc"), ("sl_traj_order", 4)])
+def test_adjoint_refuses_unsupported_forms(attr, value):
+    dt = 0.01
+    f = _flow(16, 12, 20, 2 * math.pi, math.pi, 2800.0, dt, 6)
+    setattr(f, attr, value)
+    V0 = tuple(t.clone() for t in (f.u, f.v, f.w))
+    with pytest.raises(ValueError, match="noninc"):
+        A.loss_of(f, V0, dt, 1, A.smooth_mask(f, seed=1))

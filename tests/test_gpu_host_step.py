@@ -55,3 +55,10 @@ def test_host_state_steps_match_device_steps(n3):
         assert torch.equal(hp, f.p.cpu())
         assert float(hb[0]) == float(ub) and float(hb[1]) == float(fc)
         prev, cur, nxt = cur, nxt, prev
+
+
+def test_host_state_step_refuses_incremental_pressure():
+    f = _flow(16, 12, 20, 0.01)
+    f.sl_bdf2_pressure = "inc"
+    with pytest.raises(ValueError, match="noninc"):
+        HostStateStepper(f)
