@@ -10,6 +10,9 @@ trace and gather; everything else FP64) against the FP64 oracle.
 * test_mixed_step_error_traj4: the same with tricubic trajectory sampling
   (traj_interp_order 4) against the oracle stepping with tricubic
   trajectories.
+* test_mixed_step_error_bottom_free_slip: the per-step bar with bottom-only
+  tanh stretching and a free-slip top (the FP32 locate's other branch and the
+  Neumann closure).
 * test_mixed_inc_pressure: the incremental-pressure form (bdf2_pressure inc),
   trilinear and tricubic trajectories, free-running 3 steps beside the FP64
   oracle within 1e-5.
@@ -119,6 +122,32 @@ def test_mixed_step_error_traj4(order):
             assert e < 1e-5, (step, c, e)
         div = compute_divergence(flow.u, flow.v, flow.w, n, n, n, flow.dx, flow.dy, flow.dz_f)
         assert div.abs().max().item() < 1e-11
+        assert abs(float(ub) - 1.0) < 1e-12
+        for name in ("u", "v", "w", "u_nm1", "v_nm1", "w_nm1", "p"):
+            getattr(flow, name).copy_(torch.from_numpy(getattr(ch, name)))
+
+
+@pytest.mark.parametrize("order", [6, 4])
+def test_mixed_step_error_bottom_free_slip(order):
+    n, Lx, Ly, dt, Re = 40, 2 * math.pi, math.pi, 0.02, 2800.0
+    z_f, z_c, _, _ = (t.numpy() for t in generate_grid(2.0, n, 2.0, stretching_type="bottom"))
+    u, v, w = synthetic_channel_field(n, n, n, Lx, Ly, 2.0, z_f, z_c, urms=0.12, seed=13)
+    ch = OracleChannel(n, n, n, Lx, Ly, 2.0, 2.0, 1.0 / Re, u, v, w, order=order, z_f=z_f,
+                       z_c=z_c, stretching_type="bottom", top_wall_bc_type="neumann")
+    ch.apply_bc()
+    ch.u *= 1.0 / ch.bulk_velocity()
+    ch.project_initial()
+    cfg = _config(n, Lx, Ly, order, "mixed", dt=dt)
+    cfg["domain"]["stretching_type"] = "bottom"
+    cfg["boundary_conditions"] = {"top_wall": {"type": "neumann"}}
+    flow = SLChannelFlow(config=cfg)
+    flow.set_state(*(torch.from_numpy(a) for a in (ch.u, ch.v, ch.w, ch.p)))
+    for step in range(4):
+        ch.step_bdf2(dt)
+        ub, _ = flow.step_sl_bdf2(dt)
+        for c in "uvw":
+            e = rel_err(getattr(flow, c).cpu().numpy(), getattr(ch, c))
+            assert e < 1e-5, (step, c, e)
         assert abs(float(ub) - 1.0) < 1e-12
         for name in ("u", "v", "w", "u_nm1", "v_nm1", "w_nm1", "p"):
             getattr(flow, name).copy_(torch.from_numpy(getattr(ch, name)))
