@@ -15,13 +15,13 @@ from slchannel_b200.utils import compute_bulk_velocity
 pytestmark = pytest.mark.gpu
 
 
-def _flow(nx, ny, nz, dt):
+def _flow(nx, ny, nz, dt, precision="fp64"):
     cfg = {"grid": {"nx": nx, "ny": ny, "nz": nz},
            "domain": {"Lx": 2 * math.pi, "Ly": math.pi, "Lz": 2.0},
            "flow": {"Re": 2800.0, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": 2.0},
            "initialization": {"type": "parabolic"}, "time": {"dt": dt},
            "compute": {"device": "cuda"},
-           "sl": {"interp_order": 6, "n_traj_iters": 2, "interp_dtype": "fp64"}}
+           "sl": {"interp_order": 6, "n_traj_iters": 2, "interp_dtype": precision}}
     f = SLChannelFlow(config=cfg)
     u, v, w = synthetic_channel_field(nx, ny, nz, 2 * math.pi, math.pi, 2.0, f.z_f.cpu().numpy(),
                                       f.z_c.cpu().numpy(), urms=0.1, seed=9)
@@ -33,10 +33,11 @@ def _flow(nx, ny, nz, dt):
     return f
 
 
-@pytest.mark.parametrize("n3", [(40, 32, 48), (24, 16, 20)])
-def test_host_state_steps_match_device_steps(n3):
+@pytest.mark.parametrize("n3,precision", [((40, 32, 48), "fp64"), ((24, 16, 20), "fp64"),
+                                         ((24, 16, 20), "mixed")])
+def test_host_state_steps_match_device_steps(n3, precision):
     dt = 0.02
-    f = _flow(*n3, dt)
+    f = _flow(*n3, dt, precision)
     hs = HostStateStepper(f)
     H = [tuple(pinned_like(t) for t in (f.u, f.v, f.w)) for _ in range(3)]
     for h, d in zip(H[0], (f.u_nm1, f.v_nm1, f.w_nm1)):
