@@ -1,7 +1,13 @@
 """slc_trace_gather_bdf2_staged (gather source boxes staged in shared memory
-by TMA) against slc_trace_gather_bdf2 (gather through L1): bit-identical
-outputs and clamp counts, with every box staged (small dt), with many blocks
-falling back to L1 (wide feet), and on a grid too shallow for a box."""
+by TMA) against slc_trace_gather_bdf2 (gather through L1): equal clamp counts
+and bit-identical outputs, with every box staged (small dt), with many blocks
+falling back to L1 (wide feet), and on a grid too shallow for a box.
+
+At order 4 the L1 kernel is compiled for four resident blocks per SM (64
+registers) and the staged one for two (its boxes take 78 KB of shared memory
+per block), so ptxas may fuse the shared trajectory arithmetic's multiplies
+and adds into FMAs differently in the two: there the outputs agree to
+round-off (<= 1e-13 relative), not bit for bit."""
 
 import ctypes
 import math
@@ -56,8 +62,13 @@ def _both(f, dt):
 def test_staged_equals_l1_all_staged(order):
     f = _flow((40, 24, 48), 0.01, 0.1, order)
     (a, na), (b, nb) = _both(f, 0.01)[0]
-    for x, y in zip(a, b):
-        assert torch.equal(x, y)
+    for c, x, y in zip("uvw", a, b):
+        if order == 6:
+            assert torch.equal(x, y), c
+        else:
+            e = float((x - y).abs().max() / y.abs().max())
+            print(f"order {order} {c}: staged vs L1 max relative difference {e:.3e}")
+            assert e <= 1e-13, (c, e)
     assert na == nb
     stats = _both(f, 0.01)[1]
     assert stats[0] == 0 and stats[1] > 0 and stats[2] == stats[1] and stats[3] == stats[1]
