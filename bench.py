@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     ap.add_argument("--mixed-error-steps", type=int, default=20)
+    ap.add_argument("--no-other-order", action="store_true",
+                    help="skip the FP64 step at the other interpolation order (4 <-> 6)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-channel ensemble form")
     ap.add_argument("--ensemble-n", type=int, default=48)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout check")
@@ -457,6 +459,46 @@ def measure_mixed(flow64, n, order, K, W, dist):
             "form": "FP32 fluctuation about FP64 plane means in trace+gather; rest FP64"}
 
 
+def measure_other_order(n, order, K, W):
+    """The plain FP64 step at the other interpolation order (tricubic when the
+    headline is triquintic) on the same workload: its own seeded state, BDF1
+    bootstrap, W warm-up steps, K device-timed steps."""
+    import torch
+
+    from slchannel_b200.utils import compute_divergence
+
+    other = 4 if order == 6 else 6
+    flow = build_flow(n, other)
+    for _ in range(W):
+        flow.step_sl_bdf2(DT)
+    flow._grid.timing(True)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        flow.step_sl_bdf2(DT)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    phases = flow._grid.timing_read()
+    flow._grid.timing(False)
+    div = compute_divergence(flow.u, flow.v, flow.w, n, n, n, flow.dx, flow.dy, flow.dz_f)
+    sl_ms, sl_cnt = phases["sl"]
+    _, flops_alg, pts = sl_algorithmic(n, other)
+    t_sl = sl_ms / 1000.0 / max(sl_cnt, 1)
+    out = {"order": other, "value": K / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / K,
+           "sl_kernel_ms_per_step": sl_ms / max(sl_cnt, 1),
+           "fp64_gflops": flops_alg / t_sl / 1e9,
+           "phase_ms": {p: v[0] / max(v[1], 1) for p, v in phases.items() if v[1]},
+           "max_div": float(div.abs().max()),
+           "workload": f"SL-BDF2 step {n}^3 (4pi x 2pi x 2), Re_b {RE_B}, dt {DT}, order {other}, "
+                       f"FP64, {K} steps after {W} warm-up"}
+    del flow
+    torch.cuda.empty_cache()
+    return out
+
+
 def measure_ensemble(n_inst, K, precision="fp64"):
     """The ensemble form: n_inst seeded channels (per-axis sizes from
     {32, 48, 64, 96, 128}, gamma in [1.6, 2.2], Re_b in [2000, 5000], dt at
@@ -855,6 +897,8 @@ def run_b200(args):
         "gpu_launches": int(launches), "roofline": roofline, "clocks": clocks, "e2e": e2e,
         "mixed": mixed,
     }
+    if world == 1 and not args.no_other_order:
+        line["other_order"] = measure_other_order(n, order, K, W)
     if world == 1 and not args.no_ensemble:
         line["ensemble"] = measure_ensemble(args.ensemble_n, K)
         line["ensemble_mixed"] = measure_ensemble(args.ensemble_n, K, "mixed")

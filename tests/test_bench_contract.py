@@ -93,3 +93,5 @@ def test_gpu_arm_json_line():
     assert e["value"] > 0 and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
     assert d["gpu_launches"] > 0
     assert d["mixed"]["value"] > 0 and d["mixed"]["rel_linf_err_vs_fp64"] < 1e-4
+    oo = d["other_order"]
+    assert oo["order"] == 4 and oo["value"] > 0 and oo["max_div"] < 1e-11
