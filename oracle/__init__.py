@@ -11,7 +11,8 @@ development container by ``tests/golden/make_golden.py``.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (its
 ``cpu_baseline`` leg and ``--impl reference`` arm) may import this package, and
-only as the checker or the timed CPU baseline.  The product package
+only as the reference answer that results are compared against, or as the
+timed CPU baseline.  The product package
 ``slchannel_b200`` never imports it.
 """
 

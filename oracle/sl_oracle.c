@@ -8,7 +8,8 @@
  * output agrees with the reference's eager torch path to the last few ulps.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
- * arm may load this library, and only as the checker or the timed CPU baseline;
+ * arm may load this library, and only as the reference answer that results are
+ * compared against or as the timed CPU baseline;
  * the product path (slchannel_b200) never calls it.
  *
  * Threads: POSIX threads over contiguous ranges of arrival points (each point

@@ -1,4 +1,5 @@
-"""The checkpoint format (SURVEY (f)2): slchannel_b200.utils reads the .npz
+"""The checkpoint format (the reference's fields.npz, utils.py:183-258):
+slchannel_b200.utils reads the .npz
 the reference's save_flow_fields writes (tests/golden/fields_ckpt.npz, made
 by make_checkpoint_golden.py) and writes the same keys, dtypes, shapes and
 values; the restart reader re-applies the wall ghosts as the reference's
