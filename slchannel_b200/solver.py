@@ -35,13 +35,9 @@ class SLChannelFlow:
                 config = yaml.safe_load(f)
         self.config = config
 
-        dev_cfg = config.get("compute", {}).get("device", "auto")
-        if dev_cfg == "cpu":
-            raise RuntimeError("slchannel_b200 runs on a CUDA device (sm_100a); there is no CPU path")
-        if not torch.cuda.is_available():
-            raise RuntimeError("CUDA requested but not available")
-        self.device = torch.device("cuda", torch.cuda.current_device())
-
+        # The config is checked before the device, so a bad key raises the
+        # reference's ValueError on any machine (the reference, without a GPU,
+        # falls back to its CPU device and then checks, solver.py:172-282).
         self.nx = config["grid"]["nx"]
         self.ny = config["grid"]["ny"]
         self.nz = config["grid"]["nz"]
@@ -95,6 +91,13 @@ class SLChannelFlow:
         solver_type = config.get("solver", {}).get("type", "fft")
         if solver_type != "fft":
             raise ValueError(f"solver.type must be 'fft', got {solver_type!r}.")
+
+        dev_cfg = config.get("compute", {}).get("device", "auto")
+        if dev_cfg == "cpu":
+            raise RuntimeError("slchannel_b200 runs on a CUDA device (sm_100a); there is no CPU path")
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDA requested but not available")
+        self.device = torch.device("cuda", torch.cuda.current_device())
 
         out_cfg = config.get("output", {})
         self.results_folder = out_cfg.get("results_folder", "results")
