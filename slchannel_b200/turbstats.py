@@ -18,6 +18,9 @@ accumulators once.
 
 from __future__ import annotations
 
+import os
+import warnings
+
 import numpy as np
 import torch
 
@@ -25,6 +28,7 @@ from . import _native as N
 
 PROFILES = ("U_sum", "uu_sum", "vv_sum", "ww_sum", "uw_sum", "Vm_sum", "Wm_sum", "Um2_sum",
             "Vm2_sum", "Wm2_sum", "UmWm_sum")
+SPECTRA = ("E_uu_2d_sum", "E_vv_2d_sum", "E_ww_2d_sum", "E_uw_2d_sum")
 
 
 class TurbulenceStats:
@@ -123,5 +127,74 @@ class TurbulenceStats:
         return stats
 
     def save_statistics(self, filepath):
-        """turbstats.py:464-474 -- the finalized statistics as an .npz."""
-        np.savez(filepath, **self.finalize_statistics())
+        """turbstats.py:464-473 -- the finalized statistics as a compressed .npz."""
+        np.savez_compressed(filepath, **self.finalize_statistics())
+
+    @staticmethod
+    def load_statistics(filepath):
+        """turbstats.py:475-490 -- a saved statistics file as a dict of arrays."""
+        if not os.path.exists(filepath):
+            raise FileNotFoundError(f"Statistics file not found: {filepath}")
+        data = np.load(filepath)
+        return {key: data[key] for key in data.files}
+
+    def save_state(self, filepath):
+        """turbstats.py:492-534 -- the running sums and sample counts in the
+        reference's key layout, so a run can continue the accumulation of
+        either implementation after a restart."""
+        c = lambda t: np.asarray(t.detach().cpu().numpy())  # noqa: E731
+        state = {"n_samples": self.n_samples}
+        for name in PROFILES + SPECTRA:
+            state[name] = c(getattr(self, name))
+        state.update(nx=self.nx, ny=self.ny, nz=self.nz)
+        if self.extra_planes:
+            state["n_samples_extra"] = self.n_samples_extra
+            state["spectra_z_planes"] = np.asarray(self.spectra_z_planes)
+            for pl in self.extra_planes:
+                for k in ("uu", "vv", "ww", "uw"):
+                    state[f"E_{k}_2d_z{pl['zp']:.0f}_sum"] = c(pl["sums"][k])
+        np.savez_compressed(filepath, **state)
+
+    def load_state(self, filepath):
+        """turbstats.py:536-609 -- restore the running sums written by
+        save_state (this implementation's or the reference's).  The values are
+        copied into the existing device accumulators, which the statistics
+        kernel updates in place.  Extra spectra planes are restored only when
+        the file holds the same plane set; otherwise they start at this
+        restart.  A file without the plane-mean moments (written before the
+        reference added them) leaves those at zero and warns: the normal
+        stresses of its samples are biased low by the time variance of the
+        plane mean, which cannot be recovered."""
+        if not os.path.exists(filepath):
+            raise FileNotFoundError(f"Statistics state file not found: {filepath}")
+        data = np.load(filepath)
+        if data["nx"] != self.nx or data["ny"] != self.ny or data["nz"] != self.nz:
+            raise ValueError(
+                f"Grid dimension mismatch! State file has (nx={data['nx']}, ny={data['ny']}, "
+                f"nz={data['nz']}) but current simulation has (nx={self.nx}, ny={self.ny}, "
+                f"nz={self.nz})")
+
+        def put(dst, key):
+            src = torch.as_tensor(np.asarray(data[key]), dtype=torch.float64)
+            if tuple(src.shape) != tuple(dst.shape):
+                raise ValueError(f"{key}: shape {tuple(src.shape)} in the state file, "
+                                 f"{tuple(dst.shape)} expected")
+            dst.copy_(src)
+
+        self.n_samples = int(data["n_samples"])
+        for name in ("U_sum", "uu_sum", "vv_sum", "ww_sum", "uw_sum") + SPECTRA:
+            put(getattr(self, name), name)
+        saved_planes = (list(np.asarray(data["spectra_z_planes"]).ravel())
+                        if "spectra_z_planes" in data.files else [])
+        if self.extra_planes and saved_planes == self.spectra_z_planes:
+            self.n_samples_extra = int(data["n_samples_extra"])
+            for pl in self.extra_planes:
+                for k in ("uu", "vv", "ww", "uw"):
+                    put(pl["sums"][k], f"E_{k}_2d_z{pl['zp']:.0f}_sum")
+        if "Um2_sum" in data.files:
+            for name in ("Vm_sum", "Wm_sum", "Um2_sum", "Vm2_sum", "Wm2_sum", "UmWm_sum"):
+                put(getattr(self, name), name)
+        else:
+            warnings.warn("statistics state predates the plane-mean moments: normal stresses "
+                          "of its samples are biased low by the time variance of the plane mean",
+                          RuntimeWarning, stacklevel=2)
