@@ -16,6 +16,8 @@ package.
 
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import torch
 import yaml
@@ -23,6 +25,7 @@ import yaml
 from . import _native as N
 from .initflow import initialize_flow, initialize_flow_from_file
 from .semilag import SLAdvector
+from .turbstats import TurbulenceStats
 from .utils import compute_bulk_velocity, compute_divergence, generate_grid
 
 
@@ -91,6 +94,10 @@ class SLChannelFlow:
         solver_type = config.get("solver", {}).get("type", "fft")
         if solver_type != "fft":
             raise ValueError(f"solver.type must be 'fft', got {solver_type!r}.")
+        self._stats_cfg = config.get("statistics", {}) or {}
+        self.n_stats = (self._stats_cfg.get("n_stats", 0)
+                        if self._stats_cfg.get("enabled", True) else 0)
+        self.t_stats = self._stats_cfg.get("t_stats", 10.0)
 
         dev_cfg = config.get("compute", {}).get("device", "auto")
         if dev_cfg == "cpu":
@@ -158,6 +165,28 @@ class SLChannelFlow:
         self._p_have_prev = False
         if allocate_fields:
             self._save_and_project_initial()
+
+        # Statistics (solver.py:510-550): `enabled` is an off switch and
+        # n_stats 0 also disables; restart_state_file continues an
+        # accumulation saved by save_state (this implementation's or the
+        # reference's).  The time loop that samples every n_stats steps after
+        # t_stats is the caller's.
+        self.turbulence_stats = None
+        if self.n_stats > 0:
+            self.stats_output_path = os.path.join(
+                self.results_folder, self._stats_cfg.get("output_file", "turbulence_stats.npz"))
+            self.stats_state_path = os.path.join(
+                self.results_folder,
+                self._stats_cfg.get("state_file", "turbulence_stats_state.npz"))
+            self.turbulence_stats = TurbulenceStats(
+                self.nx, self.ny, self.nz, self.Lx, self.Ly, self.Lz, self.z_c, self.z_f,
+                self.dz_c, self.dz_f, self.dx, self.dy, self.nu, self.Re_tau,
+                z_plus_target=self._stats_cfg.get("z_plus_target", 15.0), device=self.device,
+                top_wall_bc_type=self.top_wall_bc_type,
+                spectra_z_planes=self._stats_cfg.get("spectra_z_planes", None))
+            restart = self._stats_cfg.get("restart_state_file", None)
+            if restart is not None:
+                self.turbulence_stats.load_state(restart)
 
     # ------------------------------------------------------------------
     def _stream(self):
