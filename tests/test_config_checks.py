@@ -65,3 +65,22 @@ def test_every_accepted_value_passes_the_checks(path, value):
     # accepted by the checks, then refused only for the CPU device
     with pytest.raises(RuntimeError, match="no CPU path"):
         SLChannelFlow(config=_with(path, value), allocate_fields=False)
+
+
+@pytest.mark.parametrize("stats, n_stats, t_stats", [
+    (None, 0, 10.0),
+    ({"n_stats": 5}, 5, 10.0),
+    ({"n_stats": 5, "t_stats": 2.5}, 5, 2.5),
+    ({"n_stats": 5, "enabled": False}, 0, 10.0),
+    ({"enabled": True}, 0, 10.0),
+])
+def test_statistics_keys(stats, n_stats, t_stats):
+    # solver.py:510-514: `enabled` is an off switch and n_stats 0 disables;
+    # the keys are read before the device, so they can be inspected here
+    cfg = copy.deepcopy(BASE)
+    if stats is not None:
+        cfg["statistics"] = stats
+    flow = SLChannelFlow.__new__(SLChannelFlow)
+    with pytest.raises(RuntimeError, match="no CPU path"):
+        flow.__init__(config=cfg, allocate_fields=False)
+    assert flow.n_stats == n_stats and flow.t_stats == t_stats
