@@ -20,6 +20,7 @@ One JSON line on rank 0 (see the fields below).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -48,7 +49,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--n", type=int, default=256, help="grid points per direction")
+    ap.add_argument("--n", "--size", dest="n", type=int, default=256,
+                    help="grid points per direction (--size is the same option, for launchers "
+                         "such as torchrun whose own options --n abbreviates)")
     ap.add_argument("--order", type=int, default=6)
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -71,6 +74,11 @@ def parse_args():
     ap.add_argument("--report-re", type=float, default=2800.0, help="Re key (nu = 1/Re)")
     ap.add_argument("--report-dt", type=float, default=0.005)
     ap.add_argument("--report-urms", type=float, default=0.12)
+    ap.add_argument("--gather-compare", action="store_true",
+                    help="instead of the bench line: time the L1 trace+gather "
+                         "(slc_trace_gather_bdf2) against the TMA-staged one "
+                         "(slc_trace_gather_bdf2_staged) on the --n^3 benchmark state and on a "
+                         "128^3 channel at trajectory CFL 3 (JSON lines)")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0,
                     help="CPU seconds the cpu_baseline sample aims for")
     return ap.parse_args()
@@ -184,6 +192,14 @@ def config(n, order, precision="fp64"):
         "compute": {"device": "cuda"},
         "sl": {"interp_order": order, "n_traj_iters": 2, "interp_dtype": precision},
     }
+
+
+def bench_config(n, order, world):
+    """The `config` object of the JSON line -- the same for both arms."""
+    return {"workload": f"SL-BDF2 step {n}^3 (4pi x 2pi x 2), Re_b {RE_B}, dt {DT}, order {order}, "
+                        f"FP64, seeded synthetic field (u'_rms 0.1)",
+            "grid": [n, n, n], "order": order, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (state ~1.8 GB at 256^3), no flush"}
 
 
 def initial_field(n, z_f, z_c, seed=0):
@@ -319,6 +335,11 @@ def cpu_step_sample(n, order, budget_s, seed=0):
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's float64 path
+    (the oracle port: C trace+gather on all host threads, numpy elsewhere)
+    stepping the same 256^3 workload as the GPU arm -- one BDF1 bootstrap,
+    `--warmup` untimed BDF2 steps, then `--steps` timed whole BDF2 steps, each
+    timed by the wall clock.  Rank 0 only; other ranks exit 0."""
     world, rank, local = dist_env()
     if rank != 0:
         return 0
@@ -328,53 +349,32 @@ def run_reference(args):
     z_f, z_c, dz_f, dz_c = O.generate_grid(GAMMA, n, LZ)
     u, v, w = initial_field(n, z_f, z_c, 0)
     ch = O.OracleChannel(n, n, n, LX, LY, LZ, GAMMA, 1.0 / RE_B, u, v, w, order=order, z_f=z_f, z_c=z_c)
-    adv = ch.sl
-    fb = {c: adv.fill(c, f) for c, f in zip("uvw", (ch.u, ch.v, ch.w))}
+    del u, v, w
+    ch.u *= 1.0 / ch.bulk_velocity()
+    ch.project_initial()
     threads = O.max_threads()
-    nzi = {"u": n, "v": n, "w": n - 1}
-    total_pts = sum(n * n * nzi[c] for c in "uvw")
-    # the rest of the step (divergence, FFT Poisson, projection, PCR z-solve) at full size, once
-    t0 = time.perf_counter()
-    div = ch.divergence()
-    phi = O.solve_poisson_fft(div / ((2.0 / 3.0) * DT), ch.fft)
-    O.project_velocity(ch.u, ch.v, ch.w, phi, n, n, n, ch.dx, ch.dy, ch.dz_c, ch.dz_f, (2.0 / 3.0) * DT)
-    t_rest = time.perf_counter() - t0
-    a, b, cc = O.zsolve_coefficients("u", (2.0 / 3.0) * DT, n, dz_c, dz_f, 1.0 / RE_B)
-    t0 = time.perf_counter()
-    O.pcr_solve(a, b, cc, ch.u[1:2, 1 : n + 1, 1 : n + 1].reshape(n, n))
-    t_rest += 3 * (time.perf_counter() - t0) * n
-    # per timed step: trace+gather of both feet for one strip of arrival points per
-    # component, sized so the whole run stays within a few minutes
-    total_steps = args.warmup + args.steps
-    budget_per_step = max(0.05, 150.0 / max(total_steps, 1))
-    probe = n * 16
-    t0 = time.perf_counter()
-    adv.advect_comp("u", fb["u"], fb, 2 * DT, 0, probe)
-    adv.advect_comp("u", fb["u"], fb, DT, 0, probe)
-    per_pt = (time.perf_counter() - t0) / probe
-    strip = max(32, min(n * n, int(budget_per_step / (3 * per_pt))))
+    ch.step_bdf2(DT)  # BDF1 bootstrap: the timed steps are BDF2, as in the GPU arm
+    for _ in range(args.warmup):
+        ch.step_bdf2(DT)
     times = []
-    for it in range(total_steps):
+    for _ in range(args.steps):
         t0 = time.perf_counter()
-        for c in "uvw":
-            adv.advect_comp(c, fb[c], fb, 2 * DT, 0, strip)
-            adv.advect_comp(c, fb[c], fb, DT, 0, strip)
-        dt_s = time.perf_counter() - t0
-        if it >= args.warmup:
-            times.append(dt_s * total_pts / (3 * strip) + t_rest)
+        ch.step_bdf2(DT)
+        times.append(time.perf_counter() - t0)
     t_step = float(np.mean(times))
     value = 1.0 / t_step
-    sample = (f"oracle port (the CPU restatement of the reference's float64 path; C trace+gather on "
-              f"{threads} threads, numpy rest): per step, trace+gather of both feet for {strip} "
-              f"arrival points per component scaled to all {total_pts}, plus divergence + FFT "
-              f"Poisson + projection + PCR z-solve timed once at full size ({t_rest:.2f} s)")
+    sample = (f"oracle port: the CPU restatement of the reference's float64 SL-BDF2 step (C "
+              f"trace+gather on {threads} threads, numpy PCR z-solve, FFT Poisson, projection and "
+              f"bulk shift); {args.steps} whole {n}^3 BDF2 steps timed after a BDF1 bootstrap and "
+              f"{args.warmup} warm-up steps, {min(times):.2f}-{max(times):.2f} s per step.  The "
+              f"reference's own eager torch path is slower still (about 294 s per step at 256^3, "
+              f"order 6, on 8 cores), so the ratio against this port is conservative")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": f"SL-BDF2 step {n}^3 (4pi x 2pi x 2), Re_b {RE_B}, dt {DT}, "
-                               f"order {order}, FP64", "grid": [n, n, n], "order": order},
+        "config": bench_config(n, order, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -499,54 +499,74 @@ def measure_other_order(n, order, K, W):
     return out
 
 
-def measure_ensemble(n_inst, K, precision="fp64"):
+def measure_ensemble(n_inst, K, precision="fp64", world=1, rank=0):
     """The ensemble form: n_inst seeded channels (per-axis sizes from
     {32, 48, 64, 96, 128}, gamma in [1.6, 2.2], Re_b in [2000, 5000], dt at
-    trajectory CFL 3, order 6, FP64) advanced by one CUDA-graph step, against
-    the loop over the same channels' single-channel solvers."""
+    trajectory CFL 3, order 6) partitioned over the ranks by point count
+    (one rank: all of them); each rank advances its instances with one
+    CUDA-graph step per time level and no collective on the step path, and
+    the per-instance bulk velocity and forcing are gathered every 10 steps.
+    The time is the maximum over ranks.  On one GPU the loop over the same
+    channels' single-channel solvers is timed beside it."""
     import torch
 
-    from slchannel_b200.ensemble import ChannelEnsemble, ensemble_specs, loop_step, make_flow
+    from slchannel_b200.ensemble import (CudaStopwatch, EnsembleShard, drive_sharded,
+                                         ensemble_specs, loop_step)
 
     specs = ensemble_specs(n_inst, seed=4)
-    flows, dts = [], []
-    for s in specs:
-        f, dt = make_flow(s, order=6, precision=precision)
-        f.step_sl_bdf2(dt)
-        flows.append(f)
-        dts.append(dt)
-    ens = ChannelEnsemble(flows, dts, use_graph=True, autotune=True)
+    held = {}
 
-    def timed(fn, k):
-        for _ in range(3):
-            fn()
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(k):
-            fn()
-        b.record()
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / k
+    def make(indices):
+        held["shard"] = EnsembleShard(specs, indices, order=6, precision=precision)
+        return held["shard"]
 
     k = max(3, min(K, 20))
-    ms_graph = timed(ens.step, k)
-    ms_loop = timed(lambda: loop_step(flows, dts), max(3, k // 2))
-    pts = ens.points()
-    tiles = {}
-    for shape, (tk, _) in (ens.tune_ms or {}).items():
-        tiles[str(tk)] = tiles.get(str(tk), 0) + 1
+    dev = torch.device("cuda", torch.cuda.current_device())
+    mine, reports, secs = drive_sharded(specs, rank, world, k, 10, make, CudaStopwatch, warmup=3,
+                                        device=dev)
+    shard = held["shard"]
+    ms_graph = secs * 1000.0 / k
+    pts = sum(s["nx"] * s["ny"] * s["nz"] for s in specs)
+    final = reports[max(reports)]
+    ub_dev = max(abs(ub - 1.0) for ub, _ in final.values())
     out = {"value": 1000.0 / ms_graph, "unit": "ensemble steps/s", "ms_per_step": ms_graph,
-           "instances": n_inst, "points": pts,
+           "instances": n_inst, "points": pts, "ranks": world,
+           "instances_per_rank_max": max(len(p) for p in partition_instances_for(specs, world)),
            "mpoint_updates_per_s": 3 * pts / (ms_graph / 1000.0) / 1e6,
-           "loop_ms_per_step": ms_loop, "speedup_vs_loop": ms_loop / ms_graph,
-           "autotuned_tile_z_extents": tiles,
+           "max_abs_bulk_minus_1": ub_dev, "reports_at_steps": sorted(reports),
            "workload": f"{n_inst} channels, sizes from {{32,48,64,96,128}} per axis, 2pi x pi x 2, "
-                       f"gamma U[1.6,2.2], Re_b U[2000,5000], dt at trajectory CFL 3, order 6, {precision}"}
-    ens.close()
-    del flows, ens
+                       f"gamma U[1.6,2.2], Re_b U[2000,5000], dt at trajectory CFL 3, order 6, "
+                       f"{precision}; instances partitioned over {world} rank(s), no collective on "
+                       f"the step path, diagnostics gathered every 10 steps; max-rank time"}
+    if world == 1 and shard.ens is not None:
+        def timed(fn, kk):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(kk):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) / kk
+
+        ms_loop = timed(lambda: loop_step(shard.flows, shard.dts), max(3, k // 2))
+        tiles = {}
+        for shape, (tk, _) in (shard.ens.tune_ms or {}).items():
+            tiles[str(tk)] = tiles.get(str(tk), 0) + 1
+        out.update(loop_ms_per_step=ms_loop, speedup_vs_loop=ms_loop / ms_graph,
+                   autotuned_tile_z_extents=tiles)
+    shard.close()
+    del shard, held
     torch.cuda.empty_cache()
     return out
+
+
+def partition_instances_for(specs, world):
+    from slchannel_b200.ensemble import partition_instances
+
+    return partition_instances(specs, world)
 
 
 def measure_adjoint(n_dirs):
@@ -737,6 +757,55 @@ def measure_schemes():
                                          for k in ms if k.startswith("step_sl")}}
 
 
+def run_gather_compare(args):
+    """The two FP64 trace+gather entry points on the same inputs: the L1
+    gather (the step's) and the TMA-staged gather, each launched
+    `--warmup` + `--steps` times on the BDF2 state of (a) the benchmark
+    workload at --n^3 and (b) a 128^3 channel of the ensemble's recipe
+    (2pi x pi x 2, gamma 1.9, Re_b 3500) at trajectory CFL 3; device time
+    per call, staged-box counters, and the largest difference."""
+    import torch
+
+    from slchannel_b200 import _native as N
+    from slchannel_b200.ensemble import make_flow
+
+    torch.cuda.set_device(0)
+    cases = [("benchmark", build_flow(args.n, args.order), DT)]
+    spec = {"nx": 128, "ny": 128, "nz": 128, "Lx": 2 * math.pi, "Ly": math.pi, "Lz": LZ,
+            "gamma": 1.9, "Re": 3500.0, "seed": 4321, "cfl": 3.0, "urms": 0.1}
+    f, dt = make_flow(spec, order=args.order)
+    f.step_sl_bdf2(dt)
+    cases.append(("trajectory CFL 3, 128^3 (ensemble recipe)", f, dt))
+    for name, flow, dt in cases:
+        g, st = flow.sl.native, N.stream_of(flow.u)
+        cur, prev = (flow.u, flow.v, flow.w), (flow.u_nm1, flow.v_nm1, flow.w_nm1)
+        outs = {k: [torch.zeros_like(t) for t in cur] for k in ("l1", "staged")}
+        ncl = torch.zeros((), dtype=torch.int64, device=flow.device)
+        stats = (ctypes.c_int64 * 4)()
+        N.check(N.lib().slc_gather_stats(g.handle, stats, 1), g.handle)
+        res = {"case": name, "grid": [flow.nx, flow.ny, flow.nz], "dt": dt, "order": args.order}
+        for key, entry in (("l1", "slc_trace_gather_bdf2"), ("staged", "slc_trace_gather_bdf2_staged")):
+            def call():
+                g.call(entry, *[N.ptr(t) for t in cur], *[N.ptr(t) for t in prev], float(dt),
+                       *[N.ptr(t) for t in outs[key]], N.ptr(ncl), st)
+            for _ in range(max(args.warmup, 1)):
+                call()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(args.steps):
+                call()
+            b.record()
+            torch.cuda.synchronize()
+            res[f"{key}_ms_per_call"] = a.elapsed_time(b) / args.steps
+        N.check(N.lib().slc_gather_stats(g.handle, stats, 0), g.handle)
+        res["staged_stats"] = {"timeouts": stats[0], "blocks": stats[1], "near_boxes_staged": stats[2],
+                               "far_boxes_staged": stats[3]}
+        res["max_abs_diff"] = max(float((x - y).abs().max()) for x, y in zip(outs["l1"], outs["staged"]))
+        print(json.dumps(res), flush=True)
+    return 0
+
+
 def run_b200(args):
     import torch
 
@@ -884,14 +953,21 @@ def run_b200(args):
     if not args.no_mixed:
         mixed = measure_mixed(flow, n, order, K, W, dist)
 
+    # the mixed form's headline figures, compact: early in the line and again
+    # as its last key (a reader of only the line's head or tail sees them)
+    mixed_summary = None
+    if mixed is not None:
+        mixed_summary = {"steps_per_s": mixed["value"], "ms_per_step": mixed["ms_per_step"],
+                         "vs_fp64_steps_per_s": mixed["value"] / value,
+                         "rel_linf_err_vs_fp64": mixed["rel_linf_err_vs_fp64"],
+                         "rel_l2_err_vs_fp64": mixed["rel_l2_err_vs_fp64"],
+                         "after_steps": mixed["vs_fp64_after_steps"], "max_div": mixed["max_div"]}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"SL-BDF2 step {n}^3 (4pi x 2pi x 2), Re_b {RE_B}, dt {DT}, "
-                               f"order {order}, FP64 (plain drop-in form)",
-                   "grid": [n, n, n], "order": order, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (state ~1.8 GB at 256^3)"},
+        "config": bench_config(n, order, world),
+        "mixed_summary": mixed_summary,
         "mpoint_updates_per_s": value * 3 * n**3 / 1e6,
         "phase_ms": phase_ms, "max_div": max_div,
         "gpu_launches": int(launches), "roofline": roofline, "clocks": clocks, "e2e": e2e,
@@ -899,9 +975,9 @@ def run_b200(args):
     }
     if world == 1 and not args.no_other_order:
         line["other_order"] = measure_other_order(n, order, K, W)
-    if world == 1 and not args.no_ensemble:
-        line["ensemble"] = measure_ensemble(args.ensemble_n, K)
-        line["ensemble_mixed"] = measure_ensemble(args.ensemble_n, K, "mixed")
+    if not args.no_ensemble:  # every rank takes part (the instances shard over the ranks)
+        line["ensemble"] = measure_ensemble(args.ensemble_n, K, "fp64", world, rank)
+        line["ensemble_mixed"] = measure_ensemble(args.ensemble_n, K, "mixed", world, rank)
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = measure_adjoint(args.adjoint_fd_dirs)
     if world == 1 and not args.no_schemes:
@@ -910,6 +986,8 @@ def run_b200(args):
         t_cpu, desc, threads = cpu_step_sample(n, order, args.cpu_budget_s)
         line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": desc}
+    if mixed_summary is not None:
+        line["mixed_form"] = mixed_summary  # repeated as the line's last key
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -926,6 +1004,8 @@ def main():
         return run_reference(args)
     if args.mixed_report:
         return run_mixed_report(args)
+    if args.gather_compare:
+        return run_gather_compare(args)
     return run_b200(args)
 
 

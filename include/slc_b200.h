@@ -116,6 +116,25 @@ SLC_API int slc_advect(slc_grid *g, const double *fu, const double *fv, const do
                const double *mid_u, const double *mid_v, const double *mid_w, double dt,
                double *ou, double *ov, double *ow, int64_t *nclamp, void *stream);
 
+/* slc_advect with extra field triples interpolated at the same feet:
+ * every arrival point is traced once, and (fu, fv, fw) plus each of the
+ * n_extra triples extra_in[3 t + c] (c = 0 u, 1 v, 2 w; ghost-shaped) are
+ * interpolated there.  (ou, ov, ow) receive the advected triple as in
+ * slc_advect (ghost-shaped interiors); extra_out[3 t + c] receive triple t
+ * ARRIVAL-shaped and contiguous, (nx, ny, nz) for u and v and (nx, ny, nz-1)
+ * for w, z fastest.  *nclamp (device int64) receives the clamp count of the
+ * feet, counted once.  In the FP64 form up to 7 extra triples share one
+ * trace with the advected triple (more are traced again per group of 8); the
+ * mixed form packs and gathers each triple in turn at the same FP32 feet.
+ * n_extra <= SLC_MAX_EXTRA.
+ * Replaces SLAdvector.advect(..., extra_rhs) (semilag.py:584-671). */
+#define SLC_MAX_EXTRA 64
+SLC_API int slc_advect_extra(slc_grid *g, const double *fu, const double *fv, const double *fw,
+                             const double *mid_u, const double *mid_v, const double *mid_w,
+                             double dt, double *ou, double *ov, double *ow, int n_extra,
+                             const double *const *extra_in, double *const *extra_out,
+                             int64_t *nclamp, void *stream);
+
 /* Fused BDF2 predictor: both feet of every arrival point traced with
  * U* = 2 V^n - V^{n-1} (depths dt and 2 dt), V^n and V^{n-1} interpolated
  * there, and u_hat = 4/3 ubar - 1/3 ubarbar + (2/3) dt (2 R^n - R^{n-1})
@@ -141,9 +160,12 @@ SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *v
  * The step computes on an internal stream of the handle: ordered after the
  * handle's previous host-state call (and, at the first call, after work
  * already enqueued on `stream`), not after later work of the caller's, so
- * one call's compute overlaps the previous call's downloads.  Other entry
- * points that use the same handle on another stream must be ordered by the
- * caller (synchronise `stream` first).
+ * one call's compute overlaps the previous call's downloads.  So any work
+ * of another entry point on the same handle (on `stream` or any other
+ * stream) must have COMPLETED before the next host-state call is made
+ * (synchronise its stream first): the internal stream does not wait for
+ * it, and both would use the handle's workspaces.  Likewise, synchronise
+ * `stream` after a host-state call before other entry points use the handle.
  * No counterpart in the reference (its state is device- or CPU-resident). */
 SLC_API int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const double *const prev[3],
                                double *const next[3], double *p, double *bulk_out2, double U_bulk,
@@ -156,8 +178,12 @@ SLC_API int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const do
  * bit-identical to slc_trace_gather_bdf2.  Not the step's default: at the
  * 256^3 benchmark its shared-memory loads pay bank conflicts about equal to
  * the L1 path's line splits, and the padded copies cost an extra pass.
- * slc_gather_stats reports how many boxes were staged.  No counterpart in
- * the reference. */
+ * slc_gather_stats reports how many boxes were staged.  Synchronous: it
+ * waits for `stream` and returns SLC_E_CUDA if any bulk copy of this call
+ * did not complete within the kernel's bounded waits (the affected blocks
+ * gathered through L1, but a copy that lands after its block exited may have
+ * written another block's shared memory, so the results are not trusted).
+ * No counterpart in the reference. */
 SLC_API int slc_trace_gather_bdf2_staged(slc_grid *g, const double *un, const double *vn,
                                          const double *wn, const double *unm1, const double *vnm1,
                                          const double *wnm1, double dt, double *ou, double *ov,
@@ -180,9 +206,10 @@ SLC_API int slc_zsolve(slc_grid *g, double *u, double *v, double *w, double dt, 
  * kinematic viscosity, top_wall_neumann selects the free-slip top closure.
  * The Thomas tables live in one fixed device array of 6 * 1024 doubles
  * (48 KiB) that every GPU loading the library keeps until process exit, so
- * nz > 1024 is rejected with SLC_E_INVALID.  The first call on a device looks
- * up that array's address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  All calls on a device share the array and each call
+ * nz > 1024 is rejected with SLC_E_INVALID.  Each call looks up that array's
+ * address on the current device (cudaGetSymbolAddress, no allocation); the
+ * first call on a device also loads the library's device code there, so make
+ * that first call before any stream capture.  All calls on a device share the array and each call
  * rewrites it before reading it: calls that overlap on the GPU (different
  * streams, no ordering between them) race on it.  Errors are reported
  * through slc_last_error(NULL). */

@@ -63,6 +63,8 @@ SIGNATURES = {
     "slc_interp_points": ([_P, _I, _I, _P, _P, _P, _P, _L, _I, _P, _P, _P], _I),
     "slc_departure": ([_P, _I, _P, _P, _P, _D, _P, _P, _P, _P], _I),
     "slc_advect": ([_P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P], _I),
+    "slc_advect_extra": ([_P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _I, ctypes.POINTER(_P),
+                          ctypes.POINTER(_P), _P, _P], _I),
     "slc_trace_gather_bdf2": ([_P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P], _I),
     "slc_step_bdf2_host": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), _P, _P, _D,
                             _D, _P], _I),
@@ -248,5 +250,8 @@ def fma_peak_gflops(fp64=True, stream=None):
 
 
 def ptr_array(tensors):
-    arr = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in tensors])
+    """A C array of the tensors' device pointers (any length) and the ctypes
+    object that keeps it alive."""
+    tensors = list(tensors)
+    arr = (ctypes.c_void_p * max(len(tensors), 1))(*[t.data_ptr() for t in tensors])
     return ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p)), arr

@@ -318,7 +318,7 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
                                                const MixedView &FB, const double *__restrict__ fn,
                                                const double *__restrict__ fnm1, double dt,
                                                double *__restrict__ out, int i, int j, int k,
-                                               unsigned &ncl)
+                                               unsigned &ncl, OutMap om = OutMap{0, 0, 0})
 {
     const int nzi = (C == 2) ? P.nz - 1 : P.nz;
     if (k < nzi && j < P.ny) {
@@ -351,24 +351,29 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
             res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
             res = res + ((2.0 / 3.0) * dt) * Rh;
         }
-        const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
-        out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
+        if (MODE == 0 && om.sx != 0) {
+            out[om.off + (long long)i * om.sx + (long long)j * om.sy + k] = res;
+        } else {
+            const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
+            out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
+        }
     }
 }
 
+// om: where MODE 0 stores its results (ghost-shaped when om.sx == 0).
 template <int C, int O, int MODE, int TO>
 __global__ void __launch_bounds__(kThreads, SLC_SLM_MIN_BLOCKS)
     k_sl_mixed(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3M M,
                const __grid_constant__ MixedView FA, const __grid_constant__ MixedView FB,
                const double *__restrict__ fn,
                const double *__restrict__ fnm1, double dt, double *__restrict__ out,
-               unsigned long long *nclamp)
+               unsigned long long *nclamp, const OutMap om)
 {
     const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
     const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
     const int i = blockIdx.z;
     unsigned ncl = 0;
-    sl_point_mixed<C, O, MODE, TO>(P, M, FA, FB, fn, fnm1, dt, out, i, j, k, ncl);
+    sl_point_mixed<C, O, MODE, TO>(P, M, FA, FB, fn, fnm1, dt, out, i, j, k, ncl, om);
     add_clamps(nclamp, ncl);
 }
 
@@ -669,27 +674,29 @@ MixedView mview(const MixedWS &ws, int slot, const SlcParams &P)
 
 template <int O, int MODE, int TO>
 void launch_tt(const SlcParams &P, Tri fn, Tri fnm1, const MixedWS &ws, double dt, TriMut out,
-               unsigned long long *ncl, cudaStream_t s)
+               unsigned long long *ncl, const OutMap *om, cudaStream_t s)
 {
     Vel3M M{mview(ws, 6, P), mview(ws, 7, P), mview(ws, 8, P)};
     const dim3 gc((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
     const dim3 gw((P.nz - 1 + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
+    const OutMap ghost{0, 0, 0};
     k_sl_mixed<0, O, MODE, TO><<<gc, kThreads, 0, s>>>(P, M, mview(ws, 0, P), mview(ws, 3, P), fn.u,
-                                                    fnm1.u, dt, out.u, ncl);
+                                                    fnm1.u, dt, out.u, ncl, om ? om[0] : ghost);
     k_sl_mixed<1, O, MODE, TO><<<gc, kThreads, 0, s>>>(P, M, mview(ws, 1, P), mview(ws, 4, P), fn.v,
-                                                    fnm1.v, dt, out.v, ncl);
+                                                    fnm1.v, dt, out.v, ncl, om ? om[1] : ghost);
     if (P.nz > 1)
         k_sl_mixed<2, O, MODE, TO><<<gw, kThreads, 0, s>>>(P, M, mview(ws, 2, P), mview(ws, 5, P),
-                                                        fn.w, fnm1.w, dt, out.w, ncl);
+                                                        fn.w, fnm1.w, dt, out.w, ncl,
+                                                        om ? om[2] : ghost);
     count_launches(P.nz > 1 ? 3 : 2);
 }
 
 template <int O, int MODE>
 void launch_t(const SlcParams &P, Tri fn, Tri fnm1, const MixedWS &ws, double dt, TriMut out,
-              unsigned long long *ncl, cudaStream_t s)
+              unsigned long long *ncl, const OutMap *om, cudaStream_t s)
 {
-    if (P.traj_order == 4) launch_tt<O, MODE, 4>(P, fn, fnm1, ws, dt, out, ncl, s);
-    else launch_tt<O, MODE, 2>(P, fn, fnm1, ws, dt, out, ncl, s);
+    if (P.traj_order == 4) launch_tt<O, MODE, 4>(P, fn, fnm1, ws, dt, out, ncl, om, s);
+    else launch_tt<O, MODE, 2>(P, fn, fnm1, ws, dt, out, ncl, om, s);
 }
 
 }  // namespace
@@ -737,16 +744,18 @@ cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const 
 }
 
 cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, const MixedWS &ws,
-                            double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s)
+                            double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s,
+                            const OutMap *om)
 {
+    if (mode != 0) om = nullptr;  // the predictors always write ghost-shaped interiors
     if (P.order == 4) {
-        if (mode == 0) launch_t<4, 0>(P, fn, fnm1, ws, dt, out, nclamp, s);
-        else if (mode == 1) launch_t<4, 1>(P, fn, fnm1, ws, dt, out, nclamp, s);
-        else launch_t<4, 2>(P, fn, fnm1, ws, dt, out, nclamp, s);
+        if (mode == 0) launch_t<4, 0>(P, fn, fnm1, ws, dt, out, nclamp, om, s);
+        else if (mode == 1) launch_t<4, 1>(P, fn, fnm1, ws, dt, out, nclamp, om, s);
+        else launch_t<4, 2>(P, fn, fnm1, ws, dt, out, nclamp, om, s);
     } else {
-        if (mode == 0) launch_t<6, 0>(P, fn, fnm1, ws, dt, out, nclamp, s);
-        else if (mode == 1) launch_t<6, 1>(P, fn, fnm1, ws, dt, out, nclamp, s);
-        else launch_t<6, 2>(P, fn, fnm1, ws, dt, out, nclamp, s);
+        if (mode == 0) launch_t<6, 0>(P, fn, fnm1, ws, dt, out, nclamp, om, s);
+        else if (mode == 1) launch_t<6, 1>(P, fn, fnm1, ws, dt, out, nclamp, om, s);
+        else launch_t<6, 2>(P, fn, fnm1, ws, dt, out, nclamp, om, s);
     }
     return cudaGetLastError();
 }

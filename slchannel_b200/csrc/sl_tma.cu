@@ -272,10 +272,12 @@ __global__ void __launch_bounds__(kThreads, 2)
         out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
     }
     add_clamps(nclamp, ncl);
-    // no copy may still be writing this block's shared memory when it exits
+    // no copy may still be writing this block's shared memory when it exits;
+    // a drain that gives up is counted with the other time-outs (stats[0]),
+    // which slc_trace_gather_bdf2_staged turns into an error status
     if (tid == 0) {
-        if (fit[0]) mbar_wait(barN);
-        if (fit[1]) mbar_wait(barM);
+        if (fit[0] && !mbar_wait(barN)) atomicAdd(stats, 1ull);
+        if (fit[1] && !mbar_wait(barM)) atomicAdd(stats, 1ull);
     }
 }
 

@@ -98,6 +98,86 @@ __global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_
     add_clamps(nclamp, ncl);
 }
 
+// The BDF2 predictor of all three components in one launch: block z index
+// 3 i + c is component c at x index i, so the blocks resident at any time
+// work on one or two components of neighbouring x slabs, and the U* samples
+// that the three components' traces share come from L2 instead of being
+// read from HBM once per component launch.  Per point the arithmetic is
+// k_sl's.
+struct Tri3 {
+    const double *p[3];
+};
+struct Out3 {
+    double *p[3];
+};
+
+template <int O, int TO>
+__global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_SL_MIN_BLOCKS)
+    k_sl3(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M,
+          const __grid_constant__ Tri3 fn, const __grid_constant__ Tri3 fnm1, double dt,
+          const __grid_constant__ Out3 out, unsigned long long *nclamp)
+{
+    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
+    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
+    const int c = blockIdx.z % 3, i = blockIdx.z / 3;
+    unsigned ncl = 0;
+    if (c == 0) sl_point<0, O, 2, TO>(P, M, fn.p[0], fnm1.p[0], dt, out.p[0], i, j, k, ncl);
+    else if (c == 1) sl_point<1, O, 2, TO>(P, M, fn.p[1], fnm1.p[1], dt, out.p[1], i, j, k, ncl);
+    else sl_point<2, O, 2, TO>(P, M, fn.p[2], fnm1.p[2], dt, out.p[2], i, j, k, ncl);
+    add_clamps(nclamp, ncl);
+}
+
+// One foot per arrival point of component C, shared by the F.nf fields of
+// that component: traced once through M over dt, clamped and counted once,
+// one stencil built for the foot, and every field interpolated with it
+// (SLAdvector.advect with extra_rhs interpolates each extra triple at the
+// same departure points, semilag.py:584-671).  The per-field arithmetic is
+// sl_point's MODE 0, so field 0 matches slc_advect.
+struct MultiIO {
+    const double *in[kMaxMultiFields];
+    double *out[kMaxMultiFields];
+    OutMap map[kMaxMultiFields];  // sx == 0: the ghost-shaped interior
+    int nf;
+};
+
+template <int C, int O, int TO>
+__global__ void __launch_bounds__(kThreads) k_advect_multi(const __grid_constant__ SlcParams P,
+                                                           const __grid_constant__ Vel3 M,
+                                                           const __grid_constant__ MultiIO F,
+                                                           double dt, unsigned long long *nclamp)
+{
+    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
+    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
+    const int i = blockIdx.z;
+    const int nzi = (C == 2) ? P.nz - 1 : P.nz;
+    unsigned ncl = 0;
+    if (k < nzi && j < P.ny) {
+        double xa, ya, za;
+        arrival_point<C>(P, i, j, k, xa, ya, za);
+        double us0, vs0, ws0;
+        first_sample<C, TO>(P, M, i, j, k, xa, ya, za, us0, vs0, ws0);
+        double xd, yd, zd;
+        trace_foot<TO>(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd, yd, zd);
+        if (zd < P.z_lo || zd > P.z_hi) ncl += 1;
+        const double z = clampz(P, zd);
+        const int c = face_cell(P, z);
+        const NodeView<double> V0 = ghost_view<double>(C, F.in[0], P.nx, P.ny, P.nz);
+        Stencil<O, double> st;
+        build_stencil<C, O, double>(P, V0.sx, V0.sy, xd, yd, z, c, st);
+        const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
+        for (int f = 0; f < F.nf; ++f) {
+            const NodeView<double> V = ghost_view<double>(C, F.in[f], P.nx, P.ny, P.nz);
+            const double val = gather_sum<O, double, double>(V.p, st);
+            const OutMap om = F.map[f];
+            if (om.sx != 0)
+                F.out[f][om.off + (long long)i * om.sx + (long long)j * om.sy + k] = val;
+            else
+                F.out[f][(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = val;
+        }
+    }
+    if (nclamp) add_clamps(nclamp, ncl);
+}
+
 template <int C>
 __global__ void __launch_bounds__(kThreads) k_departure(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, double dt,
                                                         double *xd, double *yd, double *zd)
@@ -247,10 +327,29 @@ void launch_sl_tt(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt
     count_launches(P.nz > 1 ? 3 : 2);
 }
 
+#ifndef SLC_SL_FUSED3
+#define SLC_SL_FUSED3 0
+#endif
+
+template <int O, int TO>
+void launch_sl3(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
+                unsigned long long *ncl, cudaStream_t s)
+{
+    const dim3 g((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, 3 * P.nx);
+    k_sl3<O, TO><<<g, kThreads, 0, s>>>(P, M, Tri3{{fn.u, fn.v, fn.w}}, Tri3{{fnm1.u, fnm1.v, fnm1.w}},
+                                        dt, Out3{{out.u, out.v, out.w}}, ncl);
+    count_launches(1);
+}
+
 template <int O, int MODE>
 void launch_sl_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
                  unsigned long long *ncl, cudaStream_t s)
 {
+    if (MODE == 2 && SLC_SL_FUSED3 && P.nz > 1) {
+        if (P.traj_order == 4) launch_sl3<O, 4>(P, M, fn, fnm1, dt, out, ncl, s);
+        else launch_sl3<O, 2>(P, M, fn, fnm1, dt, out, ncl, s);
+        return;
+    }
     if (P.traj_order == 4) launch_sl_tt<O, MODE, 4>(P, M, fn, fnm1, dt, out, ncl, s);
     else launch_sl_tt<O, MODE, 2>(P, M, fn, fnm1, dt, out, ncl, s);
 }
@@ -269,6 +368,46 @@ cudaError_t launch_sl(const SlcParams &P, int mode, Tri fn, Tri fnm1, Tri mid, b
         if (mode == 0) launch_sl_t<6, 0>(P, M, fn, fnm1, dt, out, nclamp, s);
         else if (mode == 1) launch_sl_t<6, 1>(P, M, fn, fnm1, dt, out, nclamp, s);
         else launch_sl_t<6, 2>(P, M, fn, fnm1, dt, out, nclamp, s);
+    }
+    return cudaGetLastError();
+}
+
+namespace {
+template <int O, int TO>
+void launch_multi_t(const SlcParams &P, const MultiIO *io, const Vel3 &M, double dt,
+                    unsigned long long *ncl, cudaStream_t s)
+{
+    const dim3 gc((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
+    const dim3 gw((P.nz - 1 + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, P.nx);
+    k_advect_multi<0, O, TO><<<gc, kThreads, 0, s>>>(P, M, io[0], dt, ncl);
+    k_advect_multi<1, O, TO><<<gc, kThreads, 0, s>>>(P, M, io[1], dt, ncl);
+    if (P.nz > 1) k_advect_multi<2, O, TO><<<gw, kThreads, 0, s>>>(P, M, io[2], dt, ncl);
+    count_launches(P.nz > 1 ? 3 : 2);
+}
+}  // namespace
+
+cudaError_t launch_advect_multi(const SlcParams &P, int nf, const double *const *in,
+                                double *const *out, const OutMap *maps, Tri mid, double dt,
+                                unsigned long long *nclamp, cudaStream_t s)
+{
+    if (nf < 1 || nf > kMaxMultiFields) return cudaErrorInvalidValue;
+    MultiIO io[3];
+    for (int c = 0; c < 3; ++c) {
+        io[c].nf = nf;
+        for (int f = 0; f < nf; ++f) {
+            io[c].in[f] = in[3 * f + c];
+            io[c].out[f] = out[3 * f + c];
+            io[c].map[f] = maps[3 * f + c];
+        }
+    }
+    const Vel3 M = make_vel(P, mid, false);
+    const bool t4 = P.traj_order == 4;
+    if (P.order == 4) {
+        if (t4) launch_multi_t<4, 4>(P, io, M, dt, nclamp, s);
+        else launch_multi_t<4, 2>(P, io, M, dt, nclamp, s);
+    } else {
+        if (t4) launch_multi_t<6, 4>(P, io, M, dt, nclamp, s);
+        else launch_multi_t<6, 2>(P, io, M, dt, nclamp, s);
     }
     return cudaGetLastError();
 }

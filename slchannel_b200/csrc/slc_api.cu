@@ -614,6 +614,88 @@ int slc_advect(slc_grid *g, const double *fu, const double *fv, const double *fw
     return SLC_OK;
 }
 
+int slc_advect_extra(slc_grid *g, const double *fu, const double *fv, const double *fw,
+                     const double *mid_u, const double *mid_v, const double *mid_w, double dt,
+                     double *ou, double *ov, double *ow, int n_extra,
+                     const double *const *extra_in, double *const *extra_out, int64_t *nclamp,
+                     void *stream)
+{
+    if (!g) return fail(nullptr, SLC_E_INVALID, "null handle");
+    if (!fu || !fv || !fw || !mid_u || !mid_v || !mid_w || !ou || !ov || !ow)
+        return fail(g, SLC_E_INVALID, "null pointer");
+    if (n_extra < 0 || n_extra > SLC_MAX_EXTRA)
+        return fail(g, SLC_E_INVALID, "n_extra must be in [0, " + std::to_string(SLC_MAX_EXTRA) + "]");
+    if (n_extra > 0 && (!extra_in || !extra_out)) return fail(g, SLC_E_INVALID, "null extra arrays");
+    for (int q = 0; q < 3 * n_extra; ++q)
+        if (!extra_in[q] || !extra_out[q]) return fail(g, SLC_E_INVALID, "null extra field pointer");
+    DeviceGuard dg(g->device);
+    const SlcParams &P = g->P;
+    unsigned long long *ncl = counter(g, nclamp);
+    cudaStream_t s = S(stream);
+    SLC_CK(cudaMemsetAsync(ncl, 0, sizeof(unsigned long long), s), "memset");
+    // the extras' arrival-shaped (nx, ny, nzi) outputs, z fastest
+    OutMap arr[3];
+    for (int c = 0; c < 3; ++c) {
+        const long long nzi = c == 2 ? P.nz - 1 : P.nz;
+        arr[c] = OutMap{0, (long long)P.ny * nzi, nzi};
+    }
+    long t = tim_begin(g, SLC_PHASE_SL, s);
+    if (g->mixed) {
+        // the mixed form packs each triple's FP32 fluctuations in turn; every
+        // pack uses the same trajectory velocity, so every triple is gathered
+        // at the same FP32-traced feet
+        int rc = ensure_mixed(g);
+        if (rc) return rc;
+        const Tri mid{mid_u, mid_v, mid_w};
+        SLC_CK(launch_mixed_prepare(P, Tri{fu, fv, fw}, Tri{fu, fv, fw}, mid, g->mws, s), "mixed-form pack");
+        SLC_CK(launch_sl_mixed(P, 0, Tri{fu, fv, fw}, Tri{fu, fv, fw}, g->mws, dt, TriMut{ou, ov, ow},
+                               ncl, s),
+               "mixed advect");
+        for (int e = 0; e < n_extra; ++e) {
+            const Tri f{extra_in[3 * e], extra_in[3 * e + 1], extra_in[3 * e + 2]};
+            SLC_CK(launch_mixed_prepare(P, f, f, mid, g->mws, s), "mixed-form pack");
+            SLC_CK(launch_sl_mixed(P, 0, f, f, g->mws, dt,
+                                   TriMut{extra_out[3 * e], extra_out[3 * e + 1], extra_out[3 * e + 2]},
+                                   g->ncl_scratch, s, arr),
+                   "mixed advect (extra field)");
+        }
+        tim_end(g, t, s);
+        return SLC_OK;
+    }
+    // FP64: one trace per arrival point for up to kMaxMultiFields fields; the
+    // first launch carries the advected triple and counts the clamps
+    const double *in[3 * kMaxMultiFields];
+    double *out[3 * kMaxMultiFields];
+    OutMap maps[3 * kMaxMultiFields];
+    const Tri mid{mid_u, mid_v, mid_w};
+    int e = 0;
+    bool first = true;
+    while (first || e < n_extra) {
+        int nf = 0;
+        if (first) {
+            const double *f0[3] = {fu, fv, fw};
+            double *o0[3] = {ou, ov, ow};
+            for (int c = 0; c < 3; ++c) {
+                in[c] = f0[c];
+                out[c] = o0[c];
+                maps[c] = OutMap{0, 0, 0};
+            }
+            nf = 1;
+        }
+        for (; nf < kMaxMultiFields && e < n_extra; ++nf, ++e)
+            for (int c = 0; c < 3; ++c) {
+                in[3 * nf + c] = extra_in[3 * e + c];
+                out[3 * nf + c] = extra_out[3 * e + c];
+                maps[3 * nf + c] = arr[c];
+            }
+        SLC_CK(launch_advect_multi(P, nf, in, out, maps, mid, dt, first ? ncl : nullptr, s),
+               "advect with extra fields");
+        first = false;
+    }
+    tim_end(g, t, s);
+    return SLC_OK;
+}
+
 int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *vn, const double *wn,
                           const double *unm1, const double *vnm1, const double *wnm1, double dt,
                           double *ou, double *ov, double *ow, int64_t *nclamp, void *stream)
@@ -638,7 +720,22 @@ int slc_trace_gather_bdf2_staged(slc_grid *g, const double *un, const double *vn
     DeviceGuard dg(g->device);
     const double *cur[3] = {un, vn, wn}, *prev[3] = {unm1, vnm1, wnm1};
     double *out[3] = {ou, ov, ow};
-    return do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, S(stream), true);
+    cudaStream_t s = S(stream);
+    // time-outs of the bounded mbarrier waits (counter 0), before and after
+    unsigned long long before = 0, after = 0;
+    SLC_CK(cudaStreamSynchronize(s), "staged gather: synchronise");
+    if (g->dev_flags)
+        SLC_CK(cudaMemcpy(&before, g->dev_flags, sizeof(before), cudaMemcpyDeviceToHost), "read stats");
+    int rc = do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, s, true);
+    if (rc) return rc;
+    SLC_CK(cudaStreamSynchronize(s), "staged gather: synchronise");
+    if (g->dev_flags)
+        SLC_CK(cudaMemcpy(&after, g->dev_flags, sizeof(after), cudaMemcpyDeviceToHost), "read stats");
+    if (after != before)
+        return fail(g, SLC_E_CUDA,
+                    "staged gather: " + std::to_string(after - before) +
+                        " bulk copies did not complete within the bounded waits");
+    return SLC_OK;
 }
 
 int slc_zsolve(slc_grid *g, double *u, double *v, double *w, double dt, void *stream)

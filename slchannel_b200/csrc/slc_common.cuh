@@ -80,6 +80,13 @@ __host__ __device__ inline NodeView<T> ghost_view(int C, const T *base, int nx, 
     return v;
 }
 
+// Where a one-foot result of arrival point (i, j, k) is stored:
+// out[off + i*sx + j*sy + k].  sx == 0 selects the ghost-shaped array of the
+// component (interior entry (i+1, j+1, k+1)).
+struct OutMap {
+    long long off, sx, sy;
+};
+
 template <typename T>
 __host__ __device__ inline NodeView<T> node_view(const T *base, int NY, int NZ)
 {

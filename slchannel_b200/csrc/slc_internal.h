@@ -27,6 +27,14 @@ struct TriMut {
 // false = ghost-shaped arrays.
 cudaError_t launch_sl(const SlcParams &P, int mode, Tri fn, Tri fnm1, Tri mid, bool mid_node,
                       double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s);
+// One foot per arrival point shared by nf <= kMaxMultiFields fields of one
+// component each (SLAdvector.advect with extra_rhs): field f = in[3 f + c]
+// of component c, its result at out[3 f + c][maps[3 f + c]]; the clamps of
+// the foot are added to *nclamp (none when nclamp is null).
+constexpr int kMaxMultiFields = 8;
+cudaError_t launch_advect_multi(const SlcParams &P, int nf, const double *const *in,
+                                double *const *out, const OutMap *maps, Tri mid, double dt,
+                                unsigned long long *nclamp, cudaStream_t s);
 cudaError_t launch_departure(const SlcParams &P, int comp, Tri mid_node, double dt, double *xd,
                              double *yd, double *zd, cudaStream_t s);
 cudaError_t launch_interp(const SlcParams &P, int comp, int order, const double *buf,
@@ -104,7 +112,8 @@ cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const 
                                  cudaStream_t s);
 // mode 0 one foot of A, 1 BDF1 predictor, 2 BDF2 predictor; fn/fnm1 FP64 fields for R.
 cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, const MixedWS &ws,
-                            double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s);
+                            double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s,
+                            const OutMap *om = nullptr);
 
 // ---- ensemble kernels (many independent channels, one launch per substep) ----
 // One channel as the multi-instance kernels see it.  The three time levels of

@@ -11,7 +11,6 @@
 // affine maps, and a 5-step warp scan of the per-chunk maps hands each lane
 // its incoming value.  The reference solves the same systems with parallel
 // cyclic reduction (tridiag.py:36-61); the results agree to rounding.
-#include <mutex>
 #include <string>
 
 #include "../../include/slc_b200.h"
@@ -253,30 +252,19 @@ static __device__ __align__(256) double g_zsolve_noalloc_tables[6 * kNoAllocMaxN
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-double *g_noalloc_tables[kMaxDevices] = {};
-
-// Device address of the table array on the current device; looked up once
-// per device (in host code the array's name is only a stand-in symbol).
+// Device address of the table array on the current device.  In host code the
+// array's name is only a stand-in symbol, so the address is looked up with
+// that device current -- on every call: the lookup is cheap, and an address
+// cached across calls would dangle after a cudaDeviceReset (the module is
+// loaded again, possibly elsewhere).
 int noalloc_tables(double **out)
 {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-        return slc_report_error(SLC_E_CUDA, (std::string("cudaGetDevice: ") + cudaGetErrorString(e)).c_str());
-    if (dev < 0 || dev >= kMaxDevices)
-        return slc_report_error(SLC_E_INVALID, "slc_zsolve_noalloc: device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_tables[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_zsolve_noalloc_tables);
-        if (e != cudaSuccess || !p)
-            return slc_report_error(SLC_E_CUDA, (std::string("cudaGetSymbolAddress: ") +
-                                                 cudaGetErrorString(e)).c_str());
-        g_noalloc_tables[dev] = (double *)p;
-    }
-    *out = g_noalloc_tables[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_zsolve_noalloc_tables);
+    if (e != cudaSuccess || !p)
+        return slc_report_error(SLC_E_CUDA, (std::string("cudaGetSymbolAddress: ") +
+                                             cudaGetErrorString(e)).c_str());
+    *out = (double *)p;
     return SLC_OK;
 }
 

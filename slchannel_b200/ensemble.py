@@ -287,3 +287,102 @@ def gather_diagnostics(local, rank_instances, world, group=None):
     for part in out:
         merged.update(part)
     return dict(sorted(merged.items()))
+
+
+def reduce_max(value, device=None):
+    """The maximum of a float over all ranks of the default group (the value
+    itself without torch.distributed).  `device`: where the reduction tensor
+    lives -- a CUDA device for NCCL, the CPU for gloo."""
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def drive_sharded(specs, rank, world, steps, report_every, make_ensemble, timer, *,
+                  warmup=3, device=None, group=None):
+    """Run rank `rank`'s share of a partitioned ensemble.
+
+    The instances are split by ``partition_instances(specs, world)``;
+    ``make_ensemble(indices)`` builds this rank's ensemble (an object with
+    ``step()`` and ``diagnostics()``, the latter a list of per-instance
+    values in the order of `indices`).  After `warmup` untimed steps the rank
+    takes `steps` steps with no collective on the step path; every
+    `report_every` steps, and after the last one, the per-instance
+    diagnostics of all ranks are gathered (``gather_diagnostics``, outside
+    the timed segments).  ``timer()`` returns a fresh stopwatch with
+    ``start()`` and ``stop() -> seconds`` (CUDA events on the GPU).
+
+    Returns ``(indices, reports, seconds)``: this rank's instances, the list
+    of gathered reports ({step: {instance: diagnostics}}), and the stepping
+    time as the maximum over ranks."""
+    mine = partition_instances(specs, world)[rank]
+    ens = make_ensemble(mine)
+    for _ in range(warmup):
+        ens.step()
+    reports = {}
+    total = 0.0
+    done = 0
+    every = max(1, int(report_every))
+    while done < steps:
+        seg = min(every - done % every, steps - done)
+        sw = timer()
+        sw.start()
+        for _ in range(seg):
+            ens.step()
+        total += sw.stop()
+        done += seg
+        if done % every == 0 or done == steps:
+            reports[done] = gather_diagnostics(ens.diagnostics(), mine, world, group=group)
+    return mine, reports, reduce_max(total, device)
+
+
+class EnsembleShard:
+    """One rank's ensemble for ``drive_sharded``: the seeded instances
+    `indices` of `specs` built as single-channel solvers, bootstrapped, and
+    handed to a ChannelEnsemble.  ``diagnostics()`` gives, per instance,
+    (u_bulk, forcing) after the last step (one host synchronisation)."""
+
+    def __init__(self, specs, indices, order=6, precision="fp64", use_graph=True, autotune=True):
+        flows, dts = [], []
+        for i in indices:
+            f, dt = make_flow(specs[i], order=order, precision=precision)
+            f.step_sl_bdf2(dt)
+            flows.append(f)
+            dts.append(dt)
+        self.ens = ChannelEnsemble(flows, dts, use_graph=use_graph, autotune=autotune) if flows else None
+        self.points = self.ens.points() if self.ens else 0
+        self.flows, self.dts = flows, dts  # the single-channel solvers (not stepped by the ensemble)
+
+    def step(self):
+        if self.ens is not None:
+            self.ens.step()
+
+    def diagnostics(self):
+        if self.ens is None:
+            return []
+        b = self.ens.bulk_out.view(-1, 2).cpu().tolist()
+        return [(float(ub), float(fo)) for ub, fo in b]
+
+    def close(self):
+        if self.ens is not None:
+            self.ens.close()
+            self.ens = None
+        self.flows = []
+
+
+class CudaStopwatch:
+    """start()/stop() -> seconds between CUDA events on the current stream."""
+
+    def start(self):
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+        self.a.record()
+
+    def stop(self):
+        self.b.record()
+        self.b.synchronize()
+        return self.a.elapsed_time(self.b) / 1000.0

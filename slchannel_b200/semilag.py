@@ -142,7 +142,8 @@ class SLAdvector:
             return torch.empty(spec.NX, spec.NY, spec.NZ, **f64)
 
         self.fbuf = {c: alloc(self.spec[c]) for c in "uvw"}
-        self.mbuf = {c: alloc(self.spec[c]) for c in "uvw"}
+        self._mbuf = {c: alloc(self.spec[c]) for c in "uvw"}
+        self._mbuf_src = None
         self.ustar = torch.zeros(nx + 1, ny + 2, nz + 2, **f64)
         self.vstar = torch.zeros(nx + 2, ny + 1, nz + 2, **f64)
         self.wstar = torch.zeros(nx + 2, ny + 2, nz + 1, **f64)
@@ -164,6 +165,19 @@ class SLAdvector:
         N.require(u, (nx + 1, ny + 2, nz + 2), f"{what} u")
         N.require(v, (nx + 2, ny + 1, nz + 2), f"{what} v")
         N.require(w, (nx + 2, ny + 2, nz + 1), f"{what} w")
+
+    @property
+    def mbuf(self):
+        """The trajectory-velocity node buffers (semilag.py:367).  The
+        reference's advect leaves them holding its last trajectory velocity;
+        the kernels here read the ghost-shaped arrays directly, so that copy
+        is made only when the buffers are read (departure_coords, _sample, or
+        a caller's _fill, which then overwrites it)."""
+        if self._mbuf_src is not None:
+            src, self._mbuf_src = self._mbuf_src, None
+            for c, f in zip("uvw", src):
+                self._fill(self._mbuf[c], c, f)
+        return self._mbuf
 
     # semilag.py:387-394 (plain copies of views)
     def _fill(self, buf, comp, field):
@@ -233,34 +247,34 @@ class SLAdvector:
         ghost-shaped buffers (ustar, vstar, wstar), interiors filled, ghosts
         not refreshed, w walls 0; overwritten by the next call.  With
         extra_rhs (a list of field triples), each triple is interpolated at
-        the same departure points and returned as a fourth element (a list of
-        interior-shaped triples)."""
+        the same departure points -- traced once, in one launch per component
+        for up to seven extra triples -- and returned as a fourth element: a
+        list of new interior-shaped (arrival-shaped) triples."""
         self._check_fields(u, v, w, "advected")
         self._check_fields(u_mid, v_mid, w_mid, "trajectory")
         dt = float(dt_t)
-        self._fill(self.mbuf["u"], "u", u_mid)
-        self._fill(self.mbuf["v"], "v", v_mid)
-        self._fill(self.mbuf["w"], "w", w_mid)
+        # the reference leaves the trajectory node buffers filled; here they
+        # are filled only if someone reads them (see the mbuf property)
+        self._mbuf_src = (u_mid, v_mid, w_mid)
         s = self._stream()
-        extras = None
-        if extra_rhs is not None:
-            extras = []
-            nx, ny, nz = self.nx, self.ny, self.nz
-            for triple in extra_rhs:
-                self._check_fields(*triple, "extra_rhs")
-                tmp = (torch.zeros_like(self.ustar), torch.zeros_like(self.vstar),
-                       torch.zeros_like(self.wstar))
-                self._grid.call("slc_advect", *[N.ptr(t) for t in triple], N.ptr(u_mid),
-                                N.ptr(v_mid), N.ptr(w_mid), dt, *[N.ptr(t) for t in tmp],
-                                N.ptr(self._scratch_count), s)
-                extras.append((tmp[0][1 : nx + 1, 1 : ny + 1, 1 : nz + 1].clone(),
-                               tmp[1][1 : nx + 1, 1 : ny + 1, 1 : nz + 1].clone(),
-                               tmp[2][1 : nx + 1, 1 : ny + 1, 1:nz].clone()))
         counter = torch.zeros((), dtype=torch.int64, device=self.device)
-        self._grid.call("slc_advect", N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(u_mid), N.ptr(v_mid),
-                        N.ptr(w_mid), dt, N.ptr(self.ustar), N.ptr(self.vstar), N.ptr(self.wstar),
-                        N.ptr(counter), s)
+        if extra_rhs is None:
+            self._grid.call("slc_advect", N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(u_mid),
+                            N.ptr(v_mid), N.ptr(w_mid), dt, N.ptr(self.ustar), N.ptr(self.vstar),
+                            N.ptr(self.wstar), N.ptr(counter), s)
+            self.n_clamped_last = counter
+            return self.ustar, self.vstar, self.wstar
+        extra_rhs = list(extra_rhs)
+        for triple in extra_rhs:
+            if len(triple) != 3:
+                raise ValueError("extra_rhs entries must be (Ru, Rv, Rw) triples")
+            self._check_fields(*triple, "extra_rhs")
+        f = dict(dtype=torch.float64, device=self.device)
+        extras = [tuple(torch.empty(self.arrival[c][3], **f) for c in "uvw") for _ in extra_rhs]
+        pin, kin = N.ptr_array([t for triple in extra_rhs for t in triple])
+        pout, kout = N.ptr_array([t for triple in extras for t in triple])
+        self._grid.call("slc_advect_extra", N.ptr(u), N.ptr(v), N.ptr(w), N.ptr(u_mid),
+                        N.ptr(v_mid), N.ptr(w_mid), dt, N.ptr(self.ustar), N.ptr(self.vstar),
+                        N.ptr(self.wstar), len(extra_rhs), pin, pout, N.ptr(counter), s)
         self.n_clamped_last = counter
-        if extras is not None:
-            return self.ustar, self.vstar, self.wstar, extras
-        return self.ustar, self.vstar, self.wstar
+        return self.ustar, self.vstar, self.wstar, extras

@@ -26,7 +26,7 @@ from . import _native as N
 from .initflow import initialize_flow, initialize_flow_from_file
 from .semilag import SLAdvector
 from .turbstats import TurbulenceStats
-from .utils import compute_bulk_velocity, compute_divergence, generate_grid
+from .utils import compute_bulk_velocity, compute_divergence, compute_u_tau, generate_grid
 
 
 class SLChannelFlow:
@@ -53,7 +53,7 @@ class SLChannelFlow:
                 f"Invalid stretching type: {self.stretching_type}. "
                 "slChannel supports 'symmetric' or 'bottom'")
         self.nu = 1.0 / config["flow"]["Re"]
-        self.Re_tau = config["flow"].get("Re_tau", 180.0)
+        self.Re_tau = config["flow"]["Re_tau"]  # required, as in solver.py:210 (KeyError)
         self.U_bulk = config["flow"]["U_bulk"]
         self.gamma = config["flow"]["gamma"]
         bc_config = config.get("boundary_conditions", {})
@@ -169,8 +169,7 @@ class SLChannelFlow:
         # Statistics (solver.py:510-550): `enabled` is an off switch and
         # n_stats 0 also disables; restart_state_file continues an
         # accumulation saved by save_state (this implementation's or the
-        # reference's).  The time loop that samples every n_stats steps after
-        # t_stats is the caller's.
+        # reference's).  run_steps samples every n_stats steps after t_stats.
         self.turbulence_stats = None
         if self.n_stats > 0:
             self.stats_output_path = os.path.join(
@@ -334,7 +333,11 @@ class SLChannelFlow:
 
     def run_steps(self, n, dt=None):
         """Advance n steps of the configured scheme at fixed dt (default:
-        time.dt); returns the last (u_bulk, forcing)."""
+        time.dt); returns the last (u_bulk, forcing).  With statistics on
+        (n_stats > 0) a snapshot is accumulated after every step whose number
+        is a multiple of n_stats once time >= t_stats, as the reference's run
+        loop samples (solver.py:1424-1436); the samples stay on the device
+        until finalize_statistics() writes them."""
         dt = self.dt if dt is None else dt
         res = None
         step = self.step_imex if self.advection_scheme == "eulerian" else self.step_sl_bdf2
@@ -342,7 +345,25 @@ class SLChannelFlow:
             res = step(dt)
             self.time += dt
             self.current_step += 1
+            if (self.turbulence_stats is not None and self.time >= self.t_stats
+                    and self.current_step % self.n_stats == 0):
+                u_tau = compute_u_tau(self.u, self.z_c, self.nu,
+                                      top_wall_bc_type=self.top_wall_bc_type)
+                self.turbulence_stats.accumulate_statistics(self.u, self.v, self.w, u_tau)
         return res
+
+    def finalize_statistics(self):
+        """Write the statistics restart state and the finalized statistics
+        to the configured files (statistics.state_file / output_file under
+        output.results_folder), as the reference does at the end of a run
+        (solver.py:1593-1599).  Returns False when nothing was sampled."""
+        ts = self.turbulence_stats
+        if ts is None or ts.n_samples == 0:
+            return False
+        os.makedirs(self.results_folder, exist_ok=True)
+        ts.save_state(self.stats_state_path)
+        ts.save_statistics(self.stats_output_path)
+        return True
 
 
 def load_config(path):

@@ -43,7 +43,9 @@ def _check_line(d):
 
 
 def test_reference_arm_json_line():
-    r = _run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1"])
+    # 64^3 keeps the whole-step timing of the oracle port to seconds here
+    r = _run([sys.executable, "bench.py", "--impl", "reference", "--n", "64", "--steps", "1",
+              "--warmup", "1"])
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)
     assert len(lines) == 1
@@ -59,7 +61,7 @@ def _free_port():
 def test_reference_arm_torchrun_rank0_only():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py",
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1"]
+           "--impl", "reference", "--size", "64", "--gpus", "2", "--steps", "1", "--warmup", "1"]
     r = _run(cmd)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)
@@ -95,3 +97,11 @@ def test_gpu_arm_json_line():
     assert d["mixed"]["value"] > 0 and d["mixed"]["rel_linf_err_vs_fp64"] < 1e-4
     oo = d["other_order"]
     assert oo["order"] == 4 and oo["value"] > 0 and oo["max_div"] < 1e-11
+    ms = d["mixed_summary"]
+    assert ms == d["mixed_form"] and list(d)[-1] == "mixed_form"
+    assert abs(ms["vs_fp64_steps_per_s"] - d["mixed"]["value"] / d["value"]) < 1e-12
+    # the reference arm states the same workload: identical config objects
+    r = _run([sys.executable, "bench.py", "--impl", "reference", "--n", "64", "--steps", "1",
+              "--warmup", "1"])
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert _json_lines(r.stdout)[0]["config"] == d["config"]

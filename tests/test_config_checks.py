@@ -12,7 +12,7 @@ BASE = {
     "grid": {"nx": 16, "ny": 16, "nz": 16},
     "domain": {"Lx": 6.283185307179586, "Ly": 3.141592653589793, "Lz": 2.0,
                "stretching_type": "symmetric"},
-    "flow": {"Re": 2800.0, "U_bulk": 1.0, "gamma": 2.0},
+    "flow": {"Re": 2800.0, "Re_tau": 180.0, "U_bulk": 1.0, "gamma": 2.0},
     "boundary_conditions": {"top_wall": {"type": "dirichlet"}},
     "time": {"dt": 0.01},
     "sl": {"interp_order": 6, "traj_interp_order": 2, "n_traj_iters": 2,
@@ -46,6 +46,15 @@ def _with(path, value):
 def test_bad_config_keys_raise_the_reference_message(path, value, msg):
     with pytest.raises(ValueError, match=msg):
         SLChannelFlow(config=_with(path, value), allocate_fields=False)
+
+
+def test_missing_re_tau_raises_key_error():
+    # solver.py:210 reads config['flow']['Re_tau'] without a default; it sets
+    # the statistics' nominal u_tau and spectra planes, so it stays required
+    cfg = copy.deepcopy(BASE)
+    del cfg["flow"]["Re_tau"]
+    with pytest.raises(KeyError, match="Re_tau"):
+        SLChannelFlow(config=cfg, allocate_fields=False)
 
 
 def test_valid_config_on_the_cpu_device_refuses_without_fallback():

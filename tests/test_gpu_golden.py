@@ -102,6 +102,63 @@ def test_advect_golden(adv_golden, order):
         assert int(adv.n_clamped_last) == int(d[f"clamp_ncl_o{order}_w{w0}"]) > 0
 
 
+@pytest.mark.parametrize("order", [4, 6])
+def test_advect_extra_rhs_golden(order):
+    """advect(..., extra_rhs=[two triples]) against the reference's own
+    (tests/golden/advect_extra.npz): the advected triple and each extra triple
+    (interior-shaped, interpolated at the same feet) at 1e-12 relative, the
+    clamp count exact (880 clamped feet in the wall case); inputs unchanged;
+    a second call returns new extra tensors."""
+    d = load_golden("advect_extra.npz")
+    nx, ny, nz = _grid(d)[:3]
+    adv = _adv(d, order)
+    f = [T(d[f"f_{c}"]) for c in "uvw"]
+    extra = [tuple(T(d[f"e{t}_{c}"]) for c in "uvw") for t in range(2)]
+    keep = [t.clone() for triple in extra for t in triple]
+    first = None
+    for name, pre, dt in (("dt0.3", "mid", 0.3), ("dt0.9", "mid", 0.9), ("clamp", "clamp_mid", 0.5)):
+        mid = [T(d[f"{pre}_{c}"]) for c in "uvw"]
+        key = f"o{order}_{name}"
+        us, vs, ws, ex = adv.advect(*f, *mid, torch.tensor(dt), extra_rhs=extra)
+        for c, o in zip("uvw", (us, vs, ws)):
+            assert rel_err(interior(c, C(o), nx, ny, nz), d[f"adv_{c}_{key}"]) < 1e-12, (name, c)
+        assert int(adv.n_clamped_last) == int(d[f"ncl_{key}"])
+        assert len(ex) == 2
+        for t, triple in enumerate(ex):
+            for c, o in zip("uvw", triple):
+                want = d[f"extra{t}_{c}_{key}"]
+                assert tuple(o.shape) == want.shape and o.is_contiguous()
+                assert rel_err(C(o), want) < 1e-12, (name, t, c)
+        if first is None:
+            first = ex
+        else:
+            assert first[0][0].data_ptr() != ex[0][0].data_ptr()
+    for a, b in zip(keep, [t for triple in extra for t in triple]):
+        assert torch.equal(a, b)
+    # without extra_rhs the result and the count are the same as with it
+    mid = [T(d[f"clamp_mid_{c}"]) for c in "uvw"]
+    outs = adv.advect(*f, *mid, 0.5)
+    assert len(outs) == 3
+    assert rel_err(interior("u", C(outs[0]), nx, ny, nz), d[f"adv_u_o{order}_clamp"]) < 1e-12
+    assert int(adv.n_clamped_last) == int(d[f"ncl_o{order}_clamp"])
+
+
+def test_advect_extra_rhs_many_triples():
+    """Ten extra triples (two trace groups in the FP64 form): each matches a
+    plain advect of that triple exactly."""
+    d = load_golden("advect_extra.npz")
+    nx, ny, nz = _grid(d)[:3]
+    adv = _adv(d, 6)
+    f = [T(d[f"f_{c}"]) for c in "uvw"]
+    mid = [T(d[f"mid_{c}"]) for c in "uvw"]
+    extra = [tuple(T(d[f"e{t % 2}_{c}"]) * (1.0 + 0.25 * t) for c in "uvw") for t in range(10)]
+    *_, ex = adv.advect(*f, *mid, 0.3, extra_rhs=extra)
+    for t, triple in enumerate(extra):
+        ref = [C(o).copy() for o in adv.advect(*triple, *mid, 0.3)]
+        for c, o, r in zip("uvw", ex[t], ref):
+            assert np.array_equal(C(o), interior(c, r, nx, ny, nz)), (t, c)
+
+
 def config_from_step_golden(s):
     nx, ny, nz, Lx, Ly, Lz, gamma, Re, dt, order = s["params"]
     return {

@@ -64,6 +64,41 @@ def test_mixed_advect_vs_fp64(order):
     assert int(adv.n_clamped_last) == 0
 
 
+@pytest.mark.parametrize("order", [4, 6])
+def test_mixed_advect_extra_rhs_vs_fp64(order):
+    """advect(..., extra_rhs=[two triples]) in the mixed form: the advected
+    triple and each extra triple within the reference's FP32 bar (5e-6) of
+    the FP64 oracle advecting that triple along the same trajectory velocity,
+    and the extras arrival-shaped."""
+    NX = NY = 32
+    NZ, LX, LZ, G = 48, 2 * math.pi, 2.0, 1.5
+    dx = LX / NX
+    z_f, z_c, _, _ = generate_grid(G, NZ, LZ)
+    zf, zc = z_f.numpy(), z_c.numpy()
+    adv = SLAdvector(NX, NY, NZ, dx, dx, LX, LX, LZ, z_f, z_c, G, order=order,
+                     interp_dtype="fp32_accum64", device=DEV)
+    ora = OracleAdvector(NX, NY, NZ, dx, dx, LX, LX, LZ, zf, zc, G, order=order)
+
+    def f(a, b):
+        return lambda X, Y, Z: np.sin(2 * math.pi * a * X / LX) * np.cos(2 * math.pi * b * Y / LX) * (1.0 + 0.3 * Z)
+
+    u = make_field("u", f(1, 1), NX, NY, NZ, dx, dx, zf, zc)
+    v = make_field("v", f(1, 2), NX, NY, NZ, dx, dx, zf, zc)
+    w = make_field("w", lambda X, Y, Z: 0 * X + 0 * Y + 0 * Z, NX, NY, NZ, dx, dx, zf, zc)
+    extra = [tuple(make_field(c, f(2, a), NX, NY, NZ, dx, dx, zf, zc) for c in "uvw") for a in (1, 3)]
+    T = lambda a: torch.from_numpy(a).to(DEV)  # noqa: E731
+    us, vs, ws, ex = adv.advect(T(u), T(v), T(w), T(u), T(v), T(w), 0.05,
+                                extra_rhs=[tuple(T(a) for a in e) for e in extra])
+    for c, a, b in zip("uvw", (us, vs, ws), ora.advect(u, v, w, u, v, w, 0.05)):
+        assert np.abs(a.cpu().numpy() - b).max() / (np.abs(b).max() or 1.0) < 5e-6, c
+    for e, got in zip(extra, ex):
+        refs = ora.advect(*e, u, v, w, 0.05)
+        for c, a, b in zip("uvw", got, refs):
+            b = b[1:NX + 1, 1:NY + 1, 1:(NZ if c == "w" else NZ + 1)]
+            assert tuple(a.shape) == b.shape
+            assert np.abs(a.cpu().numpy() - b).max() / (np.abs(b).max() or 1.0) < 5e-6, c
+
+
 def _config(n, Lx, Ly, order, precision, Re=2800.0, dt=0.01):
     return {
         "grid": {"nx": n, "ny": n, "nz": n},

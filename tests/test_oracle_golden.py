@@ -90,6 +90,30 @@ def test_advect_golden(adv_golden, order):
         assert adv.n_clamped_last == int(d[f"clamp_ncl_o{order}_w{w0}"]) > 0
 
 
+@pytest.mark.parametrize("order", [4, 6])
+def test_advect_extra_rhs_golden(order):
+    """advect(..., extra_rhs=[two triples]) of the reference: each extra triple
+    is the advection of that triple along the same trajectory velocity (the
+    same departure points), so the oracle's advect reproduces it."""
+    d = load_golden("advect_extra.npz")
+    nx, ny, nz, Lx, Ly, Lz, gamma = _grid(d)
+    adv = OracleAdvector(nx, ny, nz, Lx / nx, Ly / ny, Lx, Ly, Lz, d["z_f"], d["z_c"], gamma,
+                         order=order)
+    f = tuple(d[f"f_{c}"] for c in "uvw")
+    extra = [tuple(d[f"e{t}_{c}"] for c in "uvw") for t in range(2)]
+    for name, pre, dt in (("dt0.3", "mid", 0.3), ("dt0.9", "mid", 0.9), ("clamp", "clamp_mid", 0.5)):
+        mid = tuple(d[f"{pre}_{c}"] for c in "uvw")
+        key = f"o{order}_{name}"
+        outs = adv.advect(*f, *mid, dt)
+        for c, o in zip("uvw", outs):
+            assert rel_err(interior(c, o, nx, ny, nz), d[f"adv_{c}_{key}"]) < 1e-13
+        assert adv.n_clamped_last == int(d[f"ncl_{key}"])
+        for t, triple in enumerate(extra):
+            outs = adv.advect(*triple, *mid, dt)
+            for c, o in zip("uvw", outs):
+                assert rel_err(interior(c, o, nx, ny, nz), d[f"extra{t}_{c}_{key}"]) < 1e-13, (t, c)
+
+
 def oracle_from_step_golden(s):
     nx, ny, nz, Lx, Ly, Lz, gamma, Re, dt, order = s["params"]
     nx, ny, nz, order = int(nx), int(ny), int(nz), int(order)
