@@ -98,35 +98,6 @@ __global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_
     add_clamps(nclamp, ncl);
 }
 
-// The BDF2 predictor of all three components in one launch: block z index
-// 3 i + c is component c at x index i, so the blocks resident at any time
-// work on one or two components of neighbouring x slabs, and the U* samples
-// that the three components' traces share come from L2 instead of being
-// read from HBM once per component launch.  Per point the arithmetic is
-// k_sl's.
-struct Tri3 {
-    const double *p[3];
-};
-struct Out3 {
-    double *p[3];
-};
-
-template <int O, int TO>
-__global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_SL_MIN_BLOCKS)
-    k_sl3(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M,
-          const __grid_constant__ Tri3 fn, const __grid_constant__ Tri3 fnm1, double dt,
-          const __grid_constant__ Out3 out, unsigned long long *nclamp)
-{
-    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
-    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
-    const int c = blockIdx.z % 3, i = blockIdx.z / 3;
-    unsigned ncl = 0;
-    if (c == 0) sl_point<0, O, 2, TO>(P, M, fn.p[0], fnm1.p[0], dt, out.p[0], i, j, k, ncl);
-    else if (c == 1) sl_point<1, O, 2, TO>(P, M, fn.p[1], fnm1.p[1], dt, out.p[1], i, j, k, ncl);
-    else sl_point<2, O, 2, TO>(P, M, fn.p[2], fnm1.p[2], dt, out.p[2], i, j, k, ncl);
-    add_clamps(nclamp, ncl);
-}
-
 // One foot per arrival point of component C, shared by the F.nf fields of
 // that component: traced once through M over dt, clamped and counted once,
 // one stencil built for the foot, and every field interpolated with it
@@ -327,29 +298,10 @@ void launch_sl_tt(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt
     count_launches(P.nz > 1 ? 3 : 2);
 }
 
-#ifndef SLC_SL_FUSED3
-#define SLC_SL_FUSED3 0
-#endif
-
-template <int O, int TO>
-void launch_sl3(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
-                unsigned long long *ncl, cudaStream_t s)
-{
-    const dim3 g((P.nz + kTileK - 1) / kTileK, (P.ny + kTileJ - 1) / kTileJ, 3 * P.nx);
-    k_sl3<O, TO><<<g, kThreads, 0, s>>>(P, M, Tri3{{fn.u, fn.v, fn.w}}, Tri3{{fnm1.u, fnm1.v, fnm1.w}},
-                                        dt, Out3{{out.u, out.v, out.w}}, ncl);
-    count_launches(1);
-}
-
 template <int O, int MODE>
 void launch_sl_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, double dt, TriMut out,
                  unsigned long long *ncl, cudaStream_t s)
 {
-    if (MODE == 2 && SLC_SL_FUSED3 && P.nz > 1) {
-        if (P.traj_order == 4) launch_sl3<O, 4>(P, M, fn, fnm1, dt, out, ncl, s);
-        else launch_sl3<O, 2>(P, M, fn, fnm1, dt, out, ncl, s);
-        return;
-    }
     if (P.traj_order == 4) launch_sl_tt<O, MODE, 4>(P, M, fn, fnm1, dt, out, ncl, s);
     else launch_sl_tt<O, MODE, 2>(P, M, fn, fnm1, dt, out, ncl, s);
 }
