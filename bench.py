@@ -79,6 +79,10 @@ def parse_args():
                          "(slc_trace_gather_bdf2) against the TMA-staged one "
                          "(slc_trace_gather_bdf2_staged) on the --n^3 benchmark state and on a "
                          "128^3 channel at trajectory CFL 3 (JSON lines)")
+    ap.add_argument("--gather-probe", action="store_true",
+                    help="instead of the bench line: the order-6 FP32 gather by one thread per "
+                         "point against the tensor-core (mma.sync FP16x3) formulation on a "
+                         "synthetic --n^3 problem (slc_gather_probe; JSON line)")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0,
                     help="CPU seconds the cpu_baseline sample aims for")
     return ap.parse_args()
@@ -1006,6 +1010,17 @@ def main():
         return run_mixed_report(args)
     if args.gather_compare:
         return run_gather_compare(args)
+    if args.gather_probe:
+        import torch
+
+        from slchannel_b200 import _native as N
+
+        torch.cuda.set_device(0)
+        res = N.gather_probe(args.n, max(args.steps, 1))
+        res.update(n=args.n, points=args.n**3, reps=max(args.steps, 1),
+                   tensor_over_scalar_time=res["tensor_ms"] / res["scalar_ms"])
+        print(json.dumps(res), flush=True)
+        return 0
     return run_b200(args)
 
 

@@ -375,6 +375,18 @@ SLC_API int64_t slc_kernel_launches(void);
  * the denominator for the trace+gather kernels' arithmetic rate. */
 SLC_API int slc_fma_peak(int fp64, double *gflops, void *stream);
 
+/* A measurement of the gather formulation, not on the step path: the
+ * order-6 Lagrange gather of a synthetic FP32 field at n^3 smoothly displaced
+ * feet (n = 64, 128, 192 or 256), done by one thread per point with 216
+ * scalar loads (the mixed form's gather) and by tensor cores (mma.sync
+ * m16n8k16, FP16 hi/lo split of field and weights, three products, FP32
+ * accumulation, over the union of 16 points' stencil rows), each launched
+ * `reps` times.  out4 = (ms per scalar launch, ms per tensor-core launch,
+ * max |difference| / max |value|, tensor-core groups that fell back to the
+ * scalar gather per launch).  Allocates its own buffers; synchronous.
+ * No counterpart in the reference. */
+SLC_API int slc_gather_probe(int n, int reps, double *out4, void *stream);
+
 /* ---- Adjoint (reverse mode) of the step ----------------------------------------
  * No counterpart in the reference, which relies on torch autograd through its
  * eager path.  Gradients of a loss on the velocity with respect to earlier

@@ -88,6 +88,7 @@ SIGNATURES = {
     "slc_timing_read": ([_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_L)], _I),
     "slc_kernel_launches": ([], _L),
     "slc_gather_stats": ([_P, ctypes.POINTER(_L), _I], _I),
+    "slc_gather_probe": ([_I, _I, ctypes.POINTER(_D), _P], _I),
     "slc_diagnostics": ([_P, _P, _P, _P, _P, _P], _I),
     "slc_diagnostics_scratch_doubles": ([], _I),
     "slc_diagnostics_raw": ([_I, _I, _I, _D, _D, _P, _P, _P, _D, _I, _D, _D, _D, _P, _P, _P, _P, _P, _P], _I),
@@ -247,6 +248,17 @@ def fma_peak_gflops(fp64=True, stream=None):
     s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
     check(lib().slc_fma_peak(1 if fp64 else 0, ctypes.byref(out), ctypes.c_void_p(s)), None)
     return out.value
+
+
+def gather_probe(n=128, reps=10, stream=None):
+    """The scalar and the tensor-core formulations of the order-6 FP32
+    gather on a synthetic n^3 problem (slc_gather_probe): per-launch ms of
+    each, their largest relative difference, fallback groups per launch."""
+    out = (ctypes.c_double * 4)()
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(lib().slc_gather_probe(int(n), int(reps), out, ctypes.c_void_p(s)), None)
+    return {"scalar_ms": out[0], "tensor_ms": out[1], "max_rel_diff": out[2],
+            "fallback_groups_per_launch": out[3]}
 
 
 def ptr_array(tensors):
