@@ -26,7 +26,8 @@ from . import _native as N
 from .initflow import initialize_flow, initialize_flow_from_file
 from .semilag import SLAdvector
 from .turbstats import TurbulenceStats
-from .utils import compute_bulk_velocity, compute_divergence, compute_u_tau, generate_grid
+from .utils import (compute_bulk_velocity, compute_cfl_fused, compute_divergence, compute_u_tau,
+                    generate_grid)
 
 
 class SLChannelFlow:
@@ -65,6 +66,14 @@ class SLChannelFlow:
         self.n_steps = t.get("n_steps", 0)
         self.t_max = t.get("t_max", 1000.0)
         self.dt_update_interval = t.get("dt_update_interval", 0)
+        # adaptive dt (solver.py:222-239, 652-674); the reference requires
+        # CFL_target, here only when dt_update_interval asks for adaptation
+        self.cfl_target = t.get("CFL_target", None)
+        self.dt_max = t.get("dt_max", 0.01)
+        self.dt_min = t.get("dt_min", 0.0001)
+        self.diff_stability_C = t.get("diff_stability_C", 0.2)
+        if self.dt_update_interval > 0 and self.cfl_target is None:
+            raise KeyError("CFL_target")
 
         self.advection_scheme = config.get("advection", {}).get("scheme", "sl")
         if self.advection_scheme not in ["sl", "eulerian"]:
@@ -331,17 +340,41 @@ class SLChannelFlow:
         self._rhs_have_prev = True
         return self._apply_bulk_forcing(dt)
 
+    def compute_cfl_dt(self):
+        """solver.py:652-674 -- the adaptive dt: CFL_target over the fused CFL
+        inverse (a trajectory CFL for the SL scheme, capped by the explicit
+        x,y-diffusion bound), clamped to [dt_min, dt_max]."""
+        dti = compute_cfl_fused(self.u, self.v, self.w, self.nx, self.ny, self.nz, self.dx,
+                                self.dy, self.dz_f, self.dz_c)
+        if dti < 1e-10:
+            dti = 1.0
+        dt_new = self.cfl_target / dti
+        if self.advection_scheme == "sl":
+            dt_diff = self.diff_stability_C / (self.nu * (1.0 / self.dx**2 + 1.0 / self.dy**2))
+            dt_new = min(dt_new, dt_diff)
+        return min(max(dt_new, self.dt_min), self.dt_max)
+
     def run_steps(self, n, dt=None):
-        """Advance n steps of the configured scheme at fixed dt (default:
-        time.dt); returns the last (u_bulk, forcing).  With statistics on
-        (n_stats > 0) a snapshot is accumulated after every step whose number
-        is a multiple of n_stats once time >= t_stats, as the reference's run
-        loop samples (solver.py:1424-1436); the samples stay on the device
-        until finalize_statistics() writes them."""
-        dt = self.dt if dt is None else dt
+        """Advance n steps of the configured scheme; returns the last
+        (u_bulk, forcing).  With dt given, every step uses it.  Otherwise the
+        steps use time.dt, adapted as the reference's run loop does
+        (solver.py:1347-1353): with dt_update_interval > 0, before every step
+        whose number is a multiple of it, compute_cfl_dt() replaces time.dt
+        when it differs by more than 5 % (the SL step then re-bootstraps with
+        one BDF1 step).  With statistics on (n_stats > 0) a snapshot is
+        accumulated after every step whose number is a multiple of n_stats
+        once time >= t_stats (solver.py:1424-1436); the samples stay on the
+        device until finalize_statistics() writes them."""
+        fixed = dt
         res = None
         step = self.step_imex if self.advection_scheme == "eulerian" else self.step_sl_bdf2
         for _ in range(int(n)):
+            nxt = self.current_step + 1
+            if fixed is None and self.dt_update_interval > 0 and nxt % self.dt_update_interval == 0:
+                dt_new = self.compute_cfl_dt()
+                if abs(dt_new - self.dt) / self.dt > 0.05:
+                    self.dt = dt_new
+            dt = self.dt if fixed is None else fixed
             res = step(dt)
             self.time += dt
             self.current_step += 1

@@ -57,6 +57,18 @@ def test_missing_re_tau_raises_key_error():
         SLChannelFlow(config=cfg, allocate_fields=False)
 
 
+def test_adaptive_dt_needs_cfl_target():
+    # solver.py:222 reads time.CFL_target; here it is required only when
+    # time.dt_update_interval asks for the adaptive dt (solver.py:652-674)
+    cfg = copy.deepcopy(BASE)
+    cfg["time"]["dt_update_interval"] = 10
+    with pytest.raises(KeyError, match="CFL_target"):
+        SLChannelFlow(config=cfg, allocate_fields=False)
+    cfg["time"]["CFL_target"] = 3.0
+    with pytest.raises(RuntimeError, match="no CPU path"):
+        SLChannelFlow(config=cfg, allocate_fields=False)
+
+
 def test_valid_config_on_the_cpu_device_refuses_without_fallback():
     with pytest.raises(RuntimeError, match="no CPU path"):
         SLChannelFlow(config=copy.deepcopy(BASE), allocate_fields=False)
