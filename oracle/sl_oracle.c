@@ -20,6 +20,7 @@
 #include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
+#include <string.h>
 #include <unistd.h>
 
 #define ORC_MAX_ORDER 6
@@ -407,4 +408,92 @@ int64_t orc_advect_comp(const orc_grid *g, int comp, const double *fbuf, const d
                         const double *mv, const double *mw, double dt, double *out)
 {
     return orc_advect_comp_range(g, comp, fbuf, mu, mv, mw, dt, 0, orc_n_arrival(g, comp), out);
+}
+
+/* ---------------------------------------------------------------------------
+ * tridiag.py:36-61 pcr_solve for a batch of right-hand sides sharing the 1-D
+ * diagonals a, b, c (length n); d is (batch, n), solved in place.  The
+ * diagonals evolve the same way for every system, so their levels are
+ * computed once; each system then takes the same per-level update
+ *   d <- (d + alpha * d[i-s]) + gamma * d[i+s]    (absent neighbours 0)
+ * and x = d / b, in the reference's operation order (no contraction).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    const double *alpha, *gamma, *bfin;  /* levels x n, levels x n, n */
+    double *d;
+    int n, levels;
+} pcr_ctx;
+
+static int64_t pcr_range(void *c, int64_t r0, int64_t r1)
+{
+    pcr_ctx *p = (pcr_ctx *)c;
+    const int n = p->n;
+    double *tmp = (double *)malloc(sizeof(double) * (size_t)n);
+    if (!tmp) return -1;
+    for (int64_t r = r0; r < r1; ++r) {
+        double *d = p->d + r * (int64_t)n;
+        int s = 1;
+        for (int l = 0; l < p->levels; ++l, s *= 2) {
+            const double *al = p->alpha + (size_t)l * n, *ga = p->gamma + (size_t)l * n;
+            for (int i = 0; i < n; ++i) {
+                const double dd = i - s >= 0 ? d[i - s] : 0.0;
+                const double du = i + s < n ? d[i + s] : 0.0;
+                const double t1 = al[i] * dd;
+                const double t2 = d[i] + t1;
+                const double t3 = ga[i] * du;
+                tmp[i] = t2 + t3;
+            }
+            memcpy(d, tmp, sizeof(double) * (size_t)n);
+        }
+        for (int i = 0; i < n; ++i) d[i] = d[i] / p->bfin[i];
+    }
+    free(tmp);
+    return 0;
+}
+
+int orc_pcr_batch(const double *a0, const double *b0, const double *c0, double *d, int64_t batch,
+                  int n)
+{
+    if (n < 1 || batch < 0) return 1;
+    int levels = 0;
+    for (int s = 1; s < n; s *= 2) ++levels;
+    double *a = (double *)malloc(sizeof(double) * (size_t)n * 8);
+    double *alpha = (double *)malloc(sizeof(double) * (size_t)n * (levels + 1));
+    double *gamma = (double *)malloc(sizeof(double) * (size_t)n * (levels + 1));
+    if (!a || !alpha || !gamma) {
+        free(a); free(alpha); free(gamma);
+        return 2;
+    }
+    double *b = a + n, *c = b + n, *na = c + n, *nb = na + n, *nc = nb + n;
+    memcpy(a, a0, sizeof(double) * (size_t)n);
+    memcpy(b, b0, sizeof(double) * (size_t)n);
+    memcpy(c, c0, sizeof(double) * (size_t)n);
+    int s = 1;
+    for (int l = 0; l < levels; ++l, s *= 2) {
+        double *al = alpha + (size_t)l * n, *ga = gamma + (size_t)l * n;
+        for (int i = 0; i < n; ++i) {
+            const int dn = i - s, up = i + s;
+            const double a_dn = dn >= 0 ? a[dn] : 0.0, b_dn = dn >= 0 ? b[dn] : 1.0;
+            const double c_dn = dn >= 0 ? c[dn] : 0.0;
+            const double a_up = up < n ? a[up] : 0.0, b_up = up < n ? b[up] : 1.0;
+            const double c_up = up < n ? c[up] : 0.0;
+            const double alp = -a[i] / b_dn;
+            const double gam = -c[i] / b_up;
+            const double t1 = alp * c_dn;
+            const double t2 = b[i] + t1;
+            const double t3 = gam * a_up;
+            nb[i] = t2 + t3;
+            na[i] = alp * a_dn;
+            nc[i] = gam * c_up;
+            al[i] = alp;
+            ga[i] = gam;
+        }
+        memcpy(a, na, sizeof(double) * (size_t)n);
+        memcpy(b, nb, sizeof(double) * (size_t)n);
+        memcpy(c, nc, sizeof(double) * (size_t)n);
+    }
+    pcr_ctx ctx = {alpha, gamma, b, d, n, levels};
+    int64_t rc = parallel_for(batch, pcr_range, &ctx);
+    free(a); free(alpha); free(gamma);
+    return rc < 0 ? 3 : 0;
 }

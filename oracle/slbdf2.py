@@ -105,6 +105,8 @@ def _load():
     lib.orc_advect_comp_range.restype = i64
     lib.orc_n_arrival.argtypes = [P, ctypes.c_int]
     lib.orc_n_arrival.restype = i64
+    lib.orc_pcr_batch.argtypes = [P, P, P, P, i64, ctypes.c_int]
+    lib.orc_pcr_batch.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -395,7 +397,23 @@ def _shift(x, s, down, fill):
 
 def pcr_solve(a, b, c, d):
     """tridiag.py:36-61 -- parallel cyclic reduction, 1-D diagonals shared by
-    the batch, RHS (batch, n)."""
+    the batch, RHS (batch, n).  A (batch, n) float64 right-hand side goes to
+    the C restatement (the same operations in the same order on all host
+    threads, bit-identical to pcr_solve_numpy); anything else to numpy."""
+    if d.ndim == 2 and d.dtype == np.float64 and a.ndim == b.ndim == c.ndim == 1:
+        n = d.shape[-1]
+        out = np.array(d, dtype=np.float64, order="C", copy=True)
+        da, db, dc = (np.ascontiguousarray(x, dtype=np.float64) for x in (a, b, c))
+        if da.shape[0] == db.shape[0] == dc.shape[0] == n:
+            rc = _load().orc_pcr_batch(_ptr(da), _ptr(db), _ptr(dc), _ptr(out), out.shape[0], n)
+            if rc != 0:
+                raise RuntimeError(f"orc_pcr_batch failed ({rc})")
+            return out
+    return pcr_solve_numpy(a, b, c, d)
+
+
+def pcr_solve_numpy(a, b, c, d):
+    """tridiag.py:36-61 in numpy, any batch shape."""
     n = d.shape[-1]
     a, b, c, d = a.copy(), b.copy(), c.copy(), d.copy()
     s = 1

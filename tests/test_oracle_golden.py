@@ -179,3 +179,17 @@ def test_imex_golden(name):
         assert rel_err(ch.p, s[f"s{step}_p"]) < 1e-11
         assert abs(ub - float(s[f"s{step}_ubulk"])) < 1e-13
         assert abs(forcing - float(s[f"s{step}_forcing"])) < 1e-10
+
+
+def test_pcr_c_restatement_is_bit_identical_to_numpy():
+    """The oracle's threaded C PCR (tridiag.py:36-61) gives exactly what the
+    numpy restatement gives, for power-of-two and other sizes."""
+    from oracle.slbdf2 import pcr_solve, pcr_solve_numpy
+
+    rng = np.random.default_rng(3)
+    for n in (2, 5, 16, 63, 258):
+        a, c = 0.3 * rng.normal(size=n), 0.3 * rng.normal(size=n)
+        b = 2.0 + rng.random(n)
+        a[0] = c[-1] = 0.0
+        d = rng.normal(size=(4500, n))
+        assert np.array_equal(pcr_solve(a, b, c, d), pcr_solve_numpy(a, b, c, d)), n
