@@ -172,7 +172,8 @@ class SLAdvector:
         reference's advect leaves them holding its last trajectory velocity;
         the kernels here read the ghost-shaped arrays directly, so that copy
         is made only when the buffers are read (departure_coords, _sample, or
-        a caller's _fill, which then overwrites it)."""
+        a caller's _fill, which then overwrites it) -- from the trajectory
+        tensors of the last advect as they are at that moment."""
         if self._mbuf_src is not None:
             src, self._mbuf_src = self._mbuf_src, None
             for c, f in zip("uvw", src):
