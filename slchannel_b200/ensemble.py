@@ -344,7 +344,8 @@ class EnsembleShard:
     """One rank's ensemble for ``drive_sharded``: the seeded instances
     `indices` of `specs` built as single-channel solvers, bootstrapped, and
     handed to a ChannelEnsemble.  ``diagnostics()`` gives, per instance,
-    (u_bulk, forcing) after the last step (one host synchronisation)."""
+    (u_bulk, forcing, kinetic energy of the interior velocity) after the last
+    step (one host synchronisation)."""
 
     def __init__(self, specs, indices, order=6, precision="fp64", use_graph=True, autotune=True):
         flows, dts = [], []
@@ -364,8 +365,15 @@ class EnsembleShard:
     def diagnostics(self):
         if self.ens is None:
             return []
+        ke = []
+        for i, (nx, ny, nz) in enumerate(self.ens.shapes):
+            u, v, w = self.ens.velocity(i)
+            ke.append(0.5 * (u[1:nx + 1, 1:ny + 1, 1:nz + 1].square().sum()
+                             + v[1:nx + 1, 1:ny + 1, 1:nz + 1].square().sum()
+                             + w[1:nx + 1, 1:ny + 1, 1:nz].square().sum()))
+        ke = torch.stack(ke).cpu().tolist()
         b = self.ens.bulk_out.view(-1, 2).cpu().tolist()
-        return [(float(ub), float(fo)) for ub, fo in b]
+        return [(float(ub), float(fo), float(k)) for (ub, fo), k in zip(b, ke)]
 
     def close(self):
         if self.ens is not None:
