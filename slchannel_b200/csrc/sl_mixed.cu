@@ -20,6 +20,7 @@ constexpr int kThreads = 256;
 #define SLC_SLM_TILE_K 32
 #endif
 constexpr int kTileK = SLC_SLM_TILE_K, kTileJ = kThreads / kTileK;
+
 // resident blocks per SM the mixed trace+gather kernel is compiled for
 #ifndef SLC_SLM_MIN_BLOCKS
 #define SLC_SLM_MIN_BLOCKS 4
@@ -313,7 +314,11 @@ __device__ __forceinline__ double xy_diffusion64(const SlcParams &P, const doubl
 // MODE 0: one foot of A (advect); 1: BDF1 predictor; 2: BDF2 predictor.
 // FA/FB: the mixed views of the near (V^n) and far (V^{n-1}) fields of
 // component C; fn/fnm1: the same fields in FP64 (ghost-shaped) for R.
-template <int C, int O, int MODE, int TO = 0>
+// FAR_FIRST: trace the far foot before the near foot's gather, so the two
+// traces' loads overlap.  That pays in the persistent ensemble kernel (2 %
+// at 48 channels, where it also spills less) but not in the single-grid one
+// at its 64-register cap (52 bytes of spill, 0.8 % slower at 256^3).
+template <int C, int O, int MODE, int TO = 0, bool FAR_FIRST = false>
 __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &M, const MixedView &FA,
                                                const MixedView &FB, const double *__restrict__ fn,
                                                const double *__restrict__ fnm1, double dt,
@@ -337,6 +342,8 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
         }
         float ddx, ddy, ddz;
         trace_foot32<TO>(P, M, A, (float)(0.5 * dt), us0, vs0, ws0, ddx, ddy, ddz);
+        float fdx = 0.f, fdy = 0.f, fdz = 0.f;
+        if (MODE == 2 && FAR_FIRST) trace_foot32<TO>(P, M, A, (float)dt, us0, vs0, ws0, fdx, fdy, fdz);
         const double ubar = gather_foot32<C, O>(P, FA, A, ddx, ddy, ddz, ncl);
         double res;
         if (MODE == 0) {
@@ -344,7 +351,13 @@ __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &
         } else if (MODE == 1) {
             res = ubar + dt * xy_diffusion64<C>(P, fn, i, j, k);
         } else {
-            trace_foot32<TO>(P, M, A, (float)dt, us0, vs0, ws0, ddx, ddy, ddz);
+            if (FAR_FIRST) {
+                ddx = fdx;
+                ddy = fdy;
+                ddz = fdz;
+            } else {
+                trace_foot32<TO>(P, M, A, (float)dt, us0, vs0, ws0, ddx, ddy, ddz);
+            }
             const double ubb = gather_foot32<C, O>(P, FB, A, ddx, ddy, ddz, ncl);
             const double Rn = xy_diffusion64<C>(P, fn, i, j, k);
             const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion64<C>(P, fnm1, i, j, k);
@@ -655,9 +668,10 @@ __global__ void __launch_bounds__(kThreads, SLC_SLM_ENS_MIN_BLOCKS) k_sl_mixed_e
         const double *fnm1 = I.lev[ens_prev(ph)][w.a];
         double *out = I.lev[ens_next(ph)][w.a];
         unsigned ncl = 0;
-        if (w.a == 0) sl_point_mixed<0, O, 2, TO>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
-        else if (w.a == 1) sl_point_mixed<1, O, 2, TO>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
-        else sl_point_mixed<2, O, 2, TO>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl);
+        const OutMap ghost{0, 0, 0};
+        if (w.a == 0) sl_point_mixed<0, O, 2, TO, true>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl, ghost);
+        else if (w.a == 1) sl_point_mixed<1, O, 2, TO, true>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl, ghost);
+        else sl_point_mixed<2, O, 2, TO, true>(sP, M, FA, FB, fn, fnm1, I.dt, out, i, j, k, ncl, ghost);
         add_clamps(I.ncl, ncl);
     }
 }
