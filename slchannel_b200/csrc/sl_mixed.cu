@@ -21,6 +21,7 @@ constexpr int kThreads = 256;
 #endif
 constexpr int kTileK = SLC_SLM_TILE_K, kTileJ = kThreads / kTileK;
 
+
 // resident blocks per SM the mixed trace+gather kernel is compiled for
 #ifndef SLC_SLM_MIN_BLOCKS
 #define SLC_SLM_MIN_BLOCKS 4
@@ -317,7 +318,8 @@ __device__ __forceinline__ double xy_diffusion64(const SlcParams &P, const doubl
 // FAR_FIRST: trace the far foot before the near foot's gather, so the two
 // traces' loads overlap.  That pays in the persistent ensemble kernel (2 %
 // at 48 channels, where it also spills less) but not in the single-grid one
-// at its 64-register cap (52 bytes of spill, 0.8 % slower at 256^3).
+// at its 64-register cap (52 bytes of spill, 0.8 % slower at 256^3; at three
+// blocks per SM and 80 registers it is 7 % slower).
 template <int C, int O, int MODE, int TO = 0, bool FAR_FIRST = false>
 __device__ __forceinline__ void sl_point_mixed(const SlcParams &P, const Vel3M &M, const MixedView &FA,
                                                const MixedView &FB, const double *__restrict__ fn,

@@ -45,10 +45,15 @@ constexpr int kThreads = 256;
 constexpr int kTileK = SLC_SL_TILE_K, kTileJ = kThreads / kTileK;
 
 
+
 // One arrival point (i, j, k) of component C; out-of-range points only
 // contribute nothing.  Shared by the single-grid kernel below and the
 // persistent ensemble kernel, so both do the same arithmetic per point.
-template <int C, int O, int MODE, int TO = 0>
+// RH_FIRST: evaluate the explicit x,y diffusion (its ten loads) before the
+// trace instead of after the gathers.  Measured at 256^3: 1 % faster for the
+// tricubic kernel and for the ensemble kernel, 1 % slower for the triquintic
+// single-grid kernel, so only those two use it.
+template <int C, int O, int MODE, int TO = 0, bool RH_FIRST = false>
 __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
                                          const double *__restrict__ fn,
                                          const double *__restrict__ fnm1, double dt,
@@ -59,6 +64,11 @@ __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
     if (k < nzi && j < P.ny) {
         double xa, ya, za;
         arrival_point<C>(P, i, j, k, xa, ya, za);
+        double Rh_early = 0.0;
+        if (MODE == 2 && RH_FIRST) {
+            const double Rn = xy_diffusion<C>(P, fn, i, j, k);
+            Rh_early = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion<C>(P, fnm1, i, j, k);
+        }
         double us0, vs0, ws0;
         first_sample<C, TO>(P, M, i, j, k, xa, ya, za, us0, vs0, ws0);
 
@@ -79,8 +89,11 @@ __device__ __forceinline__ void sl_point(const SlcParams &P, const Vel3 &M,
         } else {
             const NodeView<double> Fm = ghost_view<double>(C, fnm1, P.nx, P.ny, P.nz);
             const double ubb = gather_foot<C, O>(P, Fm, xf, yf, zf, ncl);
-            const double Rn = xy_diffusion<C>(P, fn, i, j, k);
-            const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion<C>(P, fnm1, i, j, k);
+            double Rh = Rh_early;
+            if (!RH_FIRST) {
+                const double Rn = xy_diffusion<C>(P, fn, i, j, k);
+                Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion<C>(P, fnm1, i, j, k);
+            }
             res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
             res = res + ((2.0 / 3.0) * dt) * Rh;
         }
@@ -99,7 +112,7 @@ __global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_
     const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
     const int i = blockIdx.z;
     unsigned ncl = 0;
-    sl_point<C, O, MODE, TO>(P, M, fn, fnm1, dt, out, i, j, k, ncl);
+    sl_point<C, O, MODE, TO, O == 4>(P, M, fn, fnm1, dt, out, i, j, k, ncl);
     add_clamps(nclamp, ncl);
 }
 
@@ -268,9 +281,9 @@ __global__ void __launch_bounds__(kThreads, SLC_SL_ENS_MIN_BLOCKS) k_sl_ens(cons
         const double *fnm1 = I.lev[ens_prev(ph)][w.a];
         double *out = I.lev[ens_next(ph)][w.a];
         unsigned ncl = 0;
-        if (w.a == 0) sl_point<0, O, 2>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
-        else if (w.a == 1) sl_point<1, O, 2>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
-        else sl_point<2, O, 2>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
+        if (w.a == 0) sl_point<0, O, 2, 0, true>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else if (w.a == 1) sl_point<1, O, 2, 0, true>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
+        else sl_point<2, O, 2, 0, true>(sP, M, fn, fnm1, I.dt, out, i, j, k, ncl);
         add_clamps(I.ncl, ncl);
     }
 }
