@@ -802,6 +802,14 @@ def run_gather_compare(args):
             b.record()
             torch.cuda.synchronize()
             res[f"{key}_ms_per_call"] = a.elapsed_time(b) / args.steps
+            # the same calls once more with the library's phase events: the
+            # U* (and padded-copy) pass apart from the trace+gather launches
+            g.timing(True)
+            for _ in range(args.steps):
+                call()
+            ph = g.timing_read()
+            g.timing(False)
+            res[f"{key}_phases_ms"] = {p: round(ph[p][0] / args.steps, 4) for p in ("mid", "sl")}
         N.check(N.lib().slc_gather_stats(g.handle, stats, 0), g.handle)
         res["staged_stats"] = {"timeouts": stats[0], "blocks": stats[1], "near_boxes_staged": stats[2],
                                "far_boxes_staged": stats[3]}

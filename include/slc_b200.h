@@ -174,10 +174,11 @@ SLC_API int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const do
 /* slc_trace_gather_bdf2 with each block's two gather source boxes staged
  * in shared memory by the Tensor Memory Accelerator (3-D cp.async.bulk.tensor
  * loads of halo-padded node copies written with U*; FP64 handles with
- * nz >= 39, otherwise identical to slc_trace_gather_bdf2).  Results are
- * bit-identical to slc_trace_gather_bdf2.  Not the step's default: at the
- * 256^3 benchmark its shared-memory loads pay bank conflicts about equal to
- * the L1 path's line splits, and the padded copies cost an extra pass.
+ * nz >= 47, otherwise identical to slc_trace_gather_bdf2).  Results are
+ * bit-identical to slc_trace_gather_bdf2.  Not the step's default: its
+ * kernel is faster than the L1 one, but at the 256^3 benchmark the extra
+ * pass that writes the padded copies takes back the gain; where the feet
+ * spread (trajectory CFL 3) the call is the faster of the two.
  * slc_gather_stats reports how many boxes were staged.  Synchronous: it
  * waits for `stream` and returns SLC_E_CUDA if any bulk copy of this call
  * did not complete within the kernel's bounded waits (the affected blocks

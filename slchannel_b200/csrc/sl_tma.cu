@@ -4,8 +4,10 @@
 // Why: the order-6 gather issues 216 eight-byte loads per foot per arrival
 // point.  A warp's load at one stencil offset covers 32 consecutive z values
 // (256 bytes), which from L1 costs about three wavefronts (it straddles three
-// 128-byte lines at most alignments) and from shared memory two, conflict-
-// free at any alignment.  The kernel is bound by that data pipe.
+// 128-byte lines at most alignments) and from shared memory two when its
+// lanes read one row of the box.  The kernel is bound by that data pipe.
+// Lanes whose foot coordinate floors to the next row in x or y read another
+// row; the box depth keeps such lanes on their banks (kBZ below).
 //
 // How: a block is a tile of 2 (x) x 4 (y) x 32 (z) arrival points, one warp
 // per 32 z.  Every thread traces both feet (the iterated midpoint rule of
@@ -33,7 +35,11 @@ constexpr int kThreads = 256;
 #include "sl_device.cuh"
 
 constexpr int kTI = 2, kTJ = 4, kTK = 32;    // arrival tile (x, y, z)
-constexpr int kBX = 10, kBY = 12, kBZ = 40;  // staged box (x, y, z) in nodes
+// staged box (x, y, z) in nodes.  The z extent sets the row stride in shared
+// memory: 48 doubles = 384 bytes, a multiple of the 128-byte bank cycle, so
+// lanes whose stencil base moved one row in x or y keep their banks
+// (40 doubles gave 3.12 wavefronts per 8-byte load, 48 gives 2.33)
+constexpr int kBX = 10, kBY = 12, kBZ = 48;
 constexpr int kBoxElems = kBX * kBY * kBZ;
 constexpr size_t kBoxBytes = (size_t)kBoxElems * sizeof(double);
 constexpr size_t kSmemBytes = 2 * kBoxBytes + 1024;  // + alignment slack
@@ -282,35 +288,41 @@ __global__ void __launch_bounds__(kThreads, 2)
 }
 
 // U* = 2 V^n - V^{n-1} at every node (ghost-shaped, node entries only) and
-// the halo-padded node copies of V^n and V^{n-1}; one thread per padded
-// element (x fastest last: z contiguous in both layouts).
+// the halo-padded node copies of V^n and V^{n-1}.  One warp per padded
+// (x, y) row, lanes along z (contiguous in both layouts); the row's source
+// (x mod nx, y mod ny) is found once per row.
 template <int C>
-__global__ void k_mid_pack(SlcParams P, const double *__restrict__ a, const double *__restrict__ b,
-                           double ca, double cb, double *__restrict__ mid, double *__restrict__ pa,
-                           double *__restrict__ pb, int NZp)
+__global__ void __launch_bounds__(256) k_mid_pack(SlcParams P, const double *__restrict__ a,
+                                                  const double *__restrict__ b, double ca, double cb,
+                                                  double *__restrict__ mid, double *__restrict__ pa,
+                                                  double *__restrict__ pb, int NZp)
 {
     const int NZ = C < 2 ? P.nz + 2 : P.nz + 1;
     const int PX = P.nx + kBX, PY = P.ny + kBY;
-    const long long n = (long long)PX * PY * NZp;
+    const int rows = PX * PY;
     const NodeView<double> Va = ghost_view<double>(C, a, P.nx, P.ny, P.nz);
     const NodeView<double> Vb = ghost_view<double>(C, b, P.nx, P.ny, P.nz);
     double *vm = const_cast<double *>(ghost_view<double>(C, mid, P.nx, P.ny, P.nz).p);
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int z = (int)(t % NZp);
-        const long long q = t / NZp;
-        const int y = (int)(q % PY), x = (int)(q / PY);
-        if (z >= NZ) {
-            pa[t] = 0.0;
-            pb[t] = 0.0;
-            continue;
-        }
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
+         r += gridDim.x * (blockDim.x >> 5)) {
+        const int x = r / PY, y = r - x * PY;
         const int xi = x % P.nx, yj = y % P.ny;
-        const size_t g = (size_t)xi * Va.sx + (size_t)yj * Va.sy + z;
-        const double va = Va.p[g], vb = Vb.p[g];
-        pa[t] = va;
-        pb[t] = vb;
-        if (x < P.nx && y < P.ny) vm[g] = ca * va + cb * vb;
+        const size_t g = (size_t)xi * Va.sx + (size_t)yj * Va.sy;
+        const double *ra = Va.p + g, *rb = Vb.p + g;
+        double *dm = (x < P.nx && y < P.ny) ? vm + g : nullptr;
+        double *da = pa + (size_t)r * NZp, *db = pb + (size_t)r * NZp;
+#pragma unroll 4
+        for (int z = lane; z < NZp; z += 32) {
+            double va = 0.0, vb = 0.0;
+            if (z < NZ) {
+                va = ra[z];
+                vb = rb[z];
+                if (dm) dm[z] = ca * va + cb * vb;
+            }
+            da[z] = va;
+            db[z] = vb;
+        }
     }
 }
 
@@ -398,8 +410,8 @@ cudaError_t launch_mid_pack(const SlcParams &P, Tri cur, Tri prev, TriMut mid, c
     for (int c = 0; c < 3; ++c) {
         const int NZ = c < 2 ? P.nz + 2 : P.nz + 1;
         const int nzp = tma_padded_nz(NZ);
-        const long long n = (long long)tma_padded_elems(P, c);
-        long long blocks = (n + 255) / 256;
+        const long long rows = (long long)(P.nx + kBX) * (P.ny + kBY);
+        long long blocks = (rows + 7) / 8;  // 8 warps, one padded row each
         if (blocks > 148 * 16) blocks = 148 * 16;
         const double *a = c == 0 ? cur.u : (c == 1 ? cur.v : cur.w);
         const double *b = c == 0 ? prev.u : (c == 1 ? prev.v : prev.w);

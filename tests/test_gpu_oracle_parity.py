@@ -85,14 +85,14 @@ def test_parity_ragged_grid(order):
 
 @pytest.mark.parametrize("order", [6, 4])
 def test_parity_staged_gather_ragged(order):
-    """nz >= 39 takes the TMA-staged gather: partial x, y and z tiles, feet
-    across the periodic seams, both orders."""
+    """A ragged 30 x 18 x 48 grid: partial x, y and z tiles and feet across
+    the periodic seams, both orders."""
     run_parity(30, 18, 48, 2 * math.pi, math.pi, order, steps=4, dt=0.05, urms=0.15)
 
 
 def test_parity_staged_gather_wide_feet():
-    """Large dt: in many blocks the feet spread beyond the staged box and
-    those blocks gather through L1; wall clamps on both walls."""
+    """Large dt: feet several cells from their arrival points, wall clamps
+    on both walls."""
     run_parity(24, 16, 40, 2 * math.pi, math.pi, 6, steps=3, dt=0.6, urms=0.35)
 
 

@@ -4,7 +4,7 @@ and bit-identical outputs, with every box staged (small dt), with many blocks
 falling back to L1 (wide feet), and on a grid too shallow for a box.
 
 At order 4 the L1 kernel is compiled for four resident blocks per SM (64
-registers) and the staged one for two (its boxes take 78 KB of shared memory
+registers) and the staged one for two (its boxes take 92 KB of shared memory
 per block), so ptxas may fuse the shared trajectory arithmetic's multiplies
 and adds into FMAs differently in the two: there the outputs agree to
 round-off (<= 1e-13 relative), not bit for bit."""
@@ -75,7 +75,7 @@ def test_staged_equals_l1_all_staged(order):
 
 
 def test_staged_equals_l1_wide_feet():
-    f = _flow((24, 16, 40), 0.6, 0.35)
+    f = _flow((24, 16, 48), 0.6, 0.35)
     (a, na), (b, nb) = _both(f, 0.6)[0]
     for x, y in zip(a, b):
         assert torch.equal(x, y)
