@@ -958,7 +958,8 @@ def run_b200(args):
     e2e = {"value": world * Ke / (e2e_max / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "steps": Ke, "ms_per_step": e2e_max / Ke,
            "path": "HostStateStepper.step (slc_step_bdf2_host): state in pinned host memory, "
-                   "chunked copies overlapped with compute",
+                   "copies in pieces overlapped with compute, the step streamed by x slab",
+           "host_step": hs.stats(),
            "serialised_ms_per_step": serial_ms / Ke}
 
     mixed = None

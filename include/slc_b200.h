@@ -152,10 +152,14 @@ SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *v
  * uploads cur = V^n and prev = V^{n-1}, and downloads next = V^{n+1}, p and
  * bulk_out2 = (u_bulk, forcing).  All are host pointers; the device state is
  * the library's (double-buffered).  Uploads, compute and downloads overlap:
- * the copies run on two copy streams in 16 MiB chunks, and an upload whose
- * host source an earlier call is still downloading into waits for that chunk
- * only, so feeding each call's next back as the following call's cur
- * pipelines the round trip.  Returns after enqueueing; the outputs are on the
+ * the copies run on two copy streams in pieces, and an upload whose host
+ * source an earlier call is still downloading into waits for the overlapping
+ * pieces only, so feeding each call's next back as the following call's cur
+ * pipelines the round trip.  FP64 handles with nx >= 96 also stream the step
+ * itself by x slab: cur and next move slab by slab, and each slab's
+ * trace+gather starts once its neighbour slabs of cur are on the device
+ * (when its feet provably stay within them; otherwise after the last
+ * slab).  The results equal slc_step_bdf2's followed by slc_bulk_shift.  Returns after enqueueing; the outputs are on the
  * host, and the host buffers may be touched again, once `stream` completes.
  * The step computes on an internal stream of the handle: ordered after the
  * handle's previous host-state call (and, at the first call, after work
@@ -170,6 +174,14 @@ SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *v
 SLC_API int slc_step_bdf2_host(slc_grid *g, const double *const cur[3], const double *const prev[3],
                                double *const next[3], double *p, double *bulk_out2, double U_bulk,
                                double dt, void *stream);
+
+/* How the handle's host-state calls ran: out4[0] calls streamed by x slab,
+ * out4[1] calls run whole (mixed handles, nx < 96), out4[2] slabs of the last
+ * call (0 when it ran whole), out4[3] slabs of the last call whose feet left
+ * the slabs on the device when it was released, and that were recomputed
+ * after all of V^n had arrived.  Synchronises the handle's compute.  No
+ * counterpart in the reference. */
+SLC_API int slc_host_step_stats(slc_grid *g, int64_t *out4);
 
 /* slc_trace_gather_bdf2 with each block's two gather source boxes staged
  * in shared memory by the Tensor Memory Accelerator (3-D cp.async.bulk.tensor

@@ -88,6 +88,7 @@ SIGNATURES = {
     "slc_timing_read": ([_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_L)], _I),
     "slc_kernel_launches": ([], _L),
     "slc_gather_stats": ([_P, ctypes.POINTER(_L), _I], _I),
+    "slc_host_step_stats": ([_P, ctypes.POINTER(_L)], _I),
     "slc_gather_probe": ([_I, _I, ctypes.POINTER(_D), _P], _I),
     "slc_diagnostics": ([_P, _P, _P, _P, _P, _P], _I),
     "slc_diagnostics_scratch_doubles": ([], _I),

@@ -7,6 +7,7 @@
 // walked by one thread with coalesced accesses across the warp.  The
 // divergence and projection kernels transpose between that layout and the
 // z-contiguous velocity arrays through a 32 x 32 shared-memory tile.
+#include "slc_bc.cuh"
 #include "slc_internal.h"
 
 namespace {
@@ -20,9 +21,6 @@ namespace {
 struct BcCounts {
     long long a, b, c;  // x-ghost planes, y-ghost planes (x interior), z-ghost planes
 };
-
-__device__ __host__ inline int n_xghost(int C) { return C == 0 ? 1 : 2; }
-__device__ __host__ inline int n_yghost(int C) { return C == 1 ? 1 : 2; }
 
 __host__ __device__ inline BcCounts bc_counts(int C, int nx, int ny, int nz)
 {
@@ -61,39 +59,8 @@ __device__ inline void bc_one(const SlcParams &P, int C, double *f, long long t)
         I = (int)(q / ny) + 1;
         K = which == 0 ? 0 : g.Z - 1;
     }
-    // periodic sources in x and y
-    int Is = I, Js = J;
-    if (C == 0) {
-        if (I == 0) Is = nx;
-    } else {
-        if (I == 0) Is = nx;
-        else if (I == nx + 1) Is = 1;
-    }
-    if (C == 1) {
-        if (J == 0) Js = ny;
-    } else {
-        if (J == 0) Js = ny;
-        else if (J == ny + 1) Js = 1;
-    }
-    double val;
-    if (C == 2) {
-        if (K == 0 || K == nz) val = 0.0;  // impermeable walls
-        else val = f[(size_t)Is * g.Y * g.Z + (size_t)Js * g.Z + K];
-    } else if (C == 3) {  // pressure: Neumann copies in z
-        int Ks = K == 0 ? 1 : (K == nz + 1 ? nz : K);
-        val = f[(size_t)Is * g.Y * g.Z + (size_t)Js * g.Z + Ks];
-    } else {
-        double sign = 1.0;
-        int Ks = K;
-        if (K == 0) {
-            Ks = 1;
-            sign = -1.0;
-        } else if (K == nz + 1) {
-            Ks = nz;
-            sign = P.top_neumann ? 1.0 : -1.0;
-        }
-        val = sign * f[(size_t)Is * g.Y * g.Z + (size_t)Js * g.Z + Ks];
-    }
+    const BcSrc r = bc_src(C, nx, ny, nz, P.top_neumann, I, J, K);
+    const double val = r.zero ? 0.0 : r.sign * f[(size_t)r.Is * g.Y * g.Z + (size_t)r.Js * g.Z + r.Ks];
     f[(size_t)I * g.Y * g.Z + (size_t)J * g.Z + K] = val;
 }
 

@@ -116,6 +116,56 @@ __global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_
     add_clamps(nclamp, ncl);
 }
 
+// The slab-streamed forms of k_sl's BDF2 mode (host_step.cu): the same
+// per-point arithmetic (sl_point), on the x indices of one slab.  The gated
+// launch checks once per block that the feet stay within the slabs already on
+// the device (block-uniform: every block reads the same snapshot); the fix
+// launch runs the slabs whose gated launch stood down, one block per (z, y)
+// tile walking the slab's x indices.
+__device__ __forceinline__ bool slab_window_ok(const SlcParams &P, const SlabGate *gate, int slab,
+                                               double dt, double interp_bound, double limit)
+{
+    const double um = __longlong_as_double((long long)__ldcg(&gate->snap[slab]));
+    return 2.0 * dt * um * P.inv_dx * interp_bound <= limit;  // false for NaN
+}
+
+template <int C, int O, int TO>
+__global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_SL_MIN_BLOCKS)
+    k_sl_slab(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M,
+              const double *__restrict__ fn, const double *__restrict__ fnm1, double dt,
+              double *__restrict__ out, unsigned long long *nclamp, SlabGate *gate, int slab, int i0,
+              double limit)
+{
+    // a tricubic trajectory sample can exceed the node maximum (Lebesgue
+    // constant of the 4-point Lagrange basis, below 2 in 3-D); 4 bounds it
+    if (!slab_window_ok(P, gate, slab, dt, TO == 4 ? 4.0 : 1.0, limit)) {
+        if (threadIdx.x == 0) gate->deferred[slab] = 1;
+        return;
+    }
+    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
+    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
+    unsigned ncl = 0;
+    sl_point<C, O, 2, TO, O == 4>(P, M, fn, fnm1, dt, out, i0 + (int)blockIdx.z, j, k, ncl);
+    add_clamps(nclamp, ncl);
+}
+
+template <int C, int O, int TO>
+__global__ void __launch_bounds__(kThreads, O == 4 ? SLC_SL_O4_MIN_BLOCKS : SLC_SL_MIN_BLOCKS)
+    k_sl_fix(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M,
+             const double *__restrict__ fn, const double *__restrict__ fnm1, double dt,
+             double *__restrict__ out, unsigned long long *nclamp, const SlabGate *gate,
+             const __grid_constant__ SlabBounds sb)
+{
+    const int slab = blockIdx.z;
+    if (!__ldcg(&gate->deferred[slab])) return;
+    const int k = blockIdx.x * kTileK + (threadIdx.x % kTileK);
+    const int j = blockIdx.y * kTileJ + (threadIdx.x / kTileK);
+    unsigned ncl = 0;
+    for (int i = sb.b[slab]; i < sb.b[slab + 1]; ++i)
+        sl_point<C, O, 2, TO, O == 4>(P, M, fn, fnm1, dt, out, i, j, k, ncl);
+    add_clamps(nclamp, ncl);
+}
+
 // One foot per arrival point of component C, shared by the F.nf fields of
 // that component: traced once through M over dt, clamped and counted once,
 // one stencil built for the foot, and every field interpolated with it
@@ -340,6 +390,62 @@ cudaError_t launch_sl(const SlcParams &P, int mode, Tri fn, Tri fnm1, Tri mid, b
         else launch_sl_t<6, 2>(P, M, fn, fnm1, dt, out, nclamp, s);
     }
     return cudaGetLastError();
+}
+
+namespace {
+template <int O, int TO>
+void launch_slab_t(const SlcParams &P, int comp, const Vel3 &M, const double *fn, const double *fnm1,
+                   double dt, double *out, unsigned long long *ncl, SlabGate *gate, int slab, int i0,
+                   int i1, double limit, const SlabBounds *sb, cudaStream_t s)
+{
+    const int rows_k = comp == 2 ? P.nz - 1 : P.nz;
+    const unsigned zt = (unsigned)((rows_k + kTileK - 1) / kTileK), yt = (unsigned)((P.ny + kTileJ - 1) / kTileJ);
+    if (sb) {  // the fix launch: one block per (z, y) tile and slab
+        const dim3 g(zt, yt, (unsigned)sb->S);
+        if (comp == 0) k_sl_fix<0, O, TO><<<g, kThreads, 0, s>>>(P, M, fn, fnm1, dt, out, ncl, gate, *sb);
+        else if (comp == 1) k_sl_fix<1, O, TO><<<g, kThreads, 0, s>>>(P, M, fn, fnm1, dt, out, ncl, gate, *sb);
+        else k_sl_fix<2, O, TO><<<g, kThreads, 0, s>>>(P, M, fn, fnm1, dt, out, ncl, gate, *sb);
+    } else {
+        const dim3 g(zt, yt, (unsigned)(i1 - i0));
+        if (comp == 0) k_sl_slab<0, O, TO><<<g, kThreads, 0, s>>>(P, M, fn, fnm1, dt, out, ncl, gate, slab, i0, limit);
+        else if (comp == 1) k_sl_slab<1, O, TO><<<g, kThreads, 0, s>>>(P, M, fn, fnm1, dt, out, ncl, gate, slab, i0, limit);
+        else k_sl_slab<2, O, TO><<<g, kThreads, 0, s>>>(P, M, fn, fnm1, dt, out, ncl, gate, slab, i0, limit);
+    }
+    count_launches(1);
+}
+
+cudaError_t launch_slab_any(const SlcParams &P, int comp, const double *fn, const double *fnm1, Tri mid,
+                            double dt, double *out, unsigned long long *ncl, SlabGate *gate, int slab,
+                            int i0, int i1, double limit, const SlabBounds *sb, cudaStream_t s)
+{
+    if (comp < 0 || comp > 2 || (comp == 2 && P.nz <= 1)) return cudaErrorInvalidValue;
+    if (!sb && i1 <= i0) return cudaSuccess;
+    const Vel3 M = make_vel(P, mid, false);
+    const bool t4 = P.traj_order == 4;
+    if (P.order == 4) {
+        if (t4) launch_slab_t<4, 4>(P, comp, M, fn, fnm1, dt, out, ncl, gate, slab, i0, i1, limit, sb, s);
+        else launch_slab_t<4, 2>(P, comp, M, fn, fnm1, dt, out, ncl, gate, slab, i0, i1, limit, sb, s);
+    } else {
+        if (t4) launch_slab_t<6, 4>(P, comp, M, fn, fnm1, dt, out, ncl, gate, slab, i0, i1, limit, sb, s);
+        else launch_slab_t<6, 2>(P, comp, M, fn, fnm1, dt, out, ncl, gate, slab, i0, i1, limit, sb, s);
+    }
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_sl_slab(const SlcParams &P, int comp, const double *fn, const double *fnm1, Tri mid,
+                           double dt, double *out, unsigned long long *nclamp, SlabGate *gate, int slab,
+                           int i0, int i1, double limit, cudaStream_t s)
+{
+    return launch_slab_any(P, comp, fn, fnm1, mid, dt, out, nclamp, gate, slab, i0, i1, limit, nullptr, s);
+}
+
+cudaError_t launch_sl_fix(const SlcParams &P, int comp, const double *fn, const double *fnm1, Tri mid,
+                          double dt, double *out, unsigned long long *nclamp, const SlabGate *gate,
+                          const SlabBounds &sb, cudaStream_t s)
+{
+    return launch_slab_any(P, comp, fn, fnm1, mid, dt, out, nclamp, const_cast<SlabGate *>(gate), 0, 0, 0,
+                           0.0, &sb, s);
 }
 
 namespace {

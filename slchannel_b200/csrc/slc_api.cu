@@ -197,6 +197,17 @@ int ensure_mixed(slc_grid *g)
 }  // namespace
 
 int slc_grid_ensure_mixed(slc_grid *g) { return ensure_mixed(g); }
+int slc_grid_ensure_mid(slc_grid *g) { return ensure_mid(g); }
+
+// The BDF2 step after its trace+gather: the implicit z diffusion and the
+// projection of next (slc_step_bdf2's tail; the host step streams the rest).
+int slc_step_bdf2_tail(slc_grid *g, double *const next[3], double *p, double dt, cudaStream_t s)
+{
+    const double dt_eff = (2.0 / 3.0) * dt;
+    int rc = do_zsolve(g, next[0], next[1], next[2], dt_eff, s);
+    if (rc) return rc;
+    return do_project(g, next[0], next[1], next[2], p, dt_eff, dt_eff, s);
+}
 
 namespace {
 
@@ -889,10 +900,7 @@ int slc_step_bdf2(slc_grid *g, double *const cur[3], double *const prev[3], doub
     if (rc) return rc;
     rc = do_trace_gather_bdf2(g, cur, prev, dt, next, nclamp, s);
     if (rc) return rc;
-    const double dt_eff = (2.0 / 3.0) * dt;
-    rc = do_zsolve(g, next[0], next[1], next[2], dt_eff, s);
-    if (rc) return rc;
-    return do_project(g, next[0], next[1], next[2], p, dt_eff, dt_eff, s);
+    return slc_step_bdf2_tail(g, next, p, dt, s);
 }
 
 int slc_gather_stats(slc_grid *g, int64_t *out4, int reset)

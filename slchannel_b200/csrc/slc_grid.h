@@ -57,3 +57,7 @@ struct slc_grid {
 
 // Allocate the mixed form's workspace of a mixed-precision handle (slc_api.cu).
 int slc_grid_ensure_mixed(slc_grid *g);
+// Allocate the U* workspace g->mid (slc_api.cu).
+int slc_grid_ensure_mid(slc_grid *g);
+// zsolve + projection of slc_step_bdf2 after its trace+gather (slc_api.cu).
+int slc_step_bdf2_tail(slc_grid *g, double *const next[3], double *p, double dt, cudaStream_t s);

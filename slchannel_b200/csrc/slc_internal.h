@@ -208,3 +208,32 @@ cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsIte
 cudaError_t launch_sl_mixed_ens(const EnsInst *ins, const EnsItem *items, int nitems, int ph, int order,
                                 int traj,
                                 unsigned *queue, int grid, cudaStream_t s);
+
+// ---- host_step.cu: the host-state step streamed by x slab ----------------------
+// The x nodes [0, nx) are cut into S slabs at b[0] = 0 < b[1] < ... < b[S] = nx.
+// While V^n arrives slab by slab, a slab's BDF2 trace+gather is released once
+// its neighbour slabs are on the device; the launch reads snap[slab] (max |U*_u|
+// over the slabs prepared so far) and runs only when the feet of every point
+// of the slab provably stay within the prepared slabs.  Otherwise it sets
+// deferred[slab] and the slab is recomputed by launch_sl_fix after the last
+// slab has arrived, so the results never depend on the arrival order.
+constexpr int kMaxSlabs = 16;
+struct SlabGate {
+    unsigned long long umax;             // bits of max |U*_u| (NaN compares above inf)
+    unsigned long long snap[kMaxSlabs];  // umax when slab s was released
+    int deferred[kMaxSlabs];
+};
+struct SlabBounds {
+    int S;
+    int b[kMaxSlabs + 1];
+};
+// BDF2 trace+gather of component comp for arrival x indices [i0, i1) (slab
+// `slab`): runs when 2 dt max|U*_u| / dx (times the trajectory interpolant's
+// bound) <= limit nodes, else marks the slab deferred.
+cudaError_t launch_sl_slab(const SlcParams &P, int comp, const double *fn, const double *fnm1, Tri mid,
+                           double dt, double *out, unsigned long long *nclamp, SlabGate *gate, int slab,
+                           int i0, int i1, double limit, cudaStream_t s);
+// The deferred slabs of component comp, all x indices of each.
+cudaError_t launch_sl_fix(const SlcParams &P, int comp, const double *fn, const double *fnm1, Tri mid,
+                          double dt, double *out, unsigned long long *nclamp, const SlabGate *gate,
+                          const SlabBounds &sb, cudaStream_t s);

@@ -53,3 +53,13 @@ class HostStateStepper:
         self.flow._grid.call("slc_step_bdf2_host", pc, pp, pn, ctypes.c_void_p(p.data_ptr()),
                              ctypes.c_void_p(bulk2.data_ptr()), float(self.flow.U_bulk), float(dt),
                              stream)
+
+    def stats(self):
+        """How the host-state calls ran (slc_host_step_stats): calls streamed by
+        x slab, calls run whole, slabs of the last call, and slabs of the last
+        call recomputed after all of V^n arrived.  Synchronises."""
+        import ctypes
+        out = (ctypes.c_int64 * 4)()
+        N.check(N.lib().slc_host_step_stats(self.flow._grid.handle, out), self.flow._grid.handle)
+        return {"streamed_calls": out[0], "whole_calls": out[1], "slabs": out[2],
+                "deferred_slabs": out[3]}

@@ -1,12 +1,15 @@
 """slc_step_bdf2_host (state in pinned host memory, pipelined copies) against
 the device-resident step: four chained steps with the host buffers rotated
-as a caller would, bit-identical V, p and (u_bulk, forcing)."""
+as a caller would, bit-identical V, p and (u_bulk, forcing).  Grids with
+nx >= 96 take the slab-streamed path; a fast jet in one slab makes the slabs
+released after it stand down and be recomputed at the end."""
 
 import math
 
 import pytest
 import torch
 
+from slchannel_b200 import _native as N
 from slchannel_b200.fields import synthetic_channel_field
 from slchannel_b200.host import HostStateStepper, pinned_like
 from slchannel_b200.solver import SLChannelFlow
@@ -56,6 +59,64 @@ def test_host_state_steps_match_device_steps(n3, precision):
         assert torch.equal(hp, f.p.cpu())
         assert float(hb[0]) == float(ub) and float(hb[1]) == float(fc)
         prev, cur, nxt = cur, nxt, prev
+
+
+def _run_pair(f, dt, steps):
+    hs = HostStateStepper(f)
+    H = [tuple(pinned_like(t) for t in (f.u, f.v, f.w)) for _ in range(3)]
+    for h, d in zip(H[0], (f.u_nm1, f.v_nm1, f.w_nm1)):
+        h.copy_(d)
+    for h, d in zip(H[1], (f.u, f.v, f.w)):
+        h.copy_(d)
+    hp = pinned_like(f.p)
+    hb = torch.zeros(2, dtype=torch.float64).pin_memory()
+    prev, cur, nxt = H
+    stats = []
+    for step in range(steps):
+        hs.step(cur, prev, nxt, hp, hb, dt)
+        ub, fc = f.step_sl_bdf2(dt)
+        torch.cuda.current_stream().synchronize()
+        stats.append(hs.stats())
+        for a, b in zip(nxt, (f.u, f.v, f.w)):
+            assert torch.equal(a, b.cpu()), step
+        assert torch.equal(hp, f.p.cpu()), step
+        assert float(hb[0]) == float(ub) and float(hb[1]) == float(fc)
+        prev, cur, nxt = cur, nxt, prev
+    return stats
+
+
+def test_streamed_host_steps_match_device_steps():
+    # 96 x nodes: at least three slabs, feet far inside the neighbour slabs
+    dt = 0.02
+    f = _flow(96, 40, 48, dt)
+    st = _run_pair(f, dt, 4)
+    assert [s["streamed_calls"] for s in st] == [1, 2, 3, 4]
+    assert all(s["whole_calls"] == 0 and s["slabs"] >= 3 and s["deferred_slabs"] == 0 for s in st)
+
+
+def test_streamed_host_step_defers_slabs_the_feet_leave():
+    # slabs of W x nodes arrive in the order S-1, 0, 1, ..., S-2, and slab s
+    # is released once slab s+1 is there.  A jet of +40 in u over x nodes
+    # 70..89 carries feet ~30 nodes, beyond the W - 8 a released slab allows:
+    # the slabs released before the jet's first slab arrives run streamed,
+    # every later one is recomputed after the last slab; the results stay
+    # those of the device step
+    dt = 0.02
+    f = _flow(128, 24, 40, dt)
+    for t in (f.u, f.u_nm1):
+        t[70:90] += 40.0
+    # ghosts consistent again in both levels, as a step leaves them (the
+    # device step's next V^{n-1} is its V^n with the boundary conditions
+    # applied, the host caller's is the buffer it passed)
+    for tri in ((f.u, f.v, f.w), (f.u_nm1, f.v_nm1, f.w_nm1)):
+        f._grid.call("slc_apply_bc", *[N.ptr(t) for t in tri], N.stream_of(f.u))
+    st = _run_pair(f, dt, 2)
+    S = st[0]["slabs"]
+    assert S >= 3
+    jet_slab = 70 * S // 128  # slab of x node 70 (bounds floor(s * 128 / S))
+    released_before_jet = jet_slab - 1
+    assert released_before_jet >= 1
+    assert st[0]["deferred_slabs"] == S - released_before_jet, st
 
 
 def test_host_state_step_refuses_incremental_pressure():
