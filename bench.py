@@ -414,9 +414,13 @@ def measure_mixed(flow64, n, order, K, W, dist):
     copy_state(flow32, flow64)
     for _ in range(W):
         flow32.step_sl_bdf2(DT)
+    from slchannel_b200 import _native as N
+
     flow32._grid.timing(True)
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gstats = (ctypes.c_int64 * 4)()
+    N.check(N.lib().slc_gather_stats(flow32._grid.handle, gstats, 1), flow32._grid.handle)
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(K):
@@ -426,6 +430,7 @@ def measure_mixed(flow64, n, order, K, W, dist):
     ms = e0.elapsed_time(e1)
     phases = flow32._grid.timing_read()
     flow32._grid.timing(False)
+    N.check(N.lib().slc_gather_stats(flow32._grid.handle, gstats, 1), flow32._grid.handle)
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -446,8 +451,6 @@ def measure_mixed(flow64, n, order, K, W, dist):
                    / sum((getattr(flow64, c) ** 2).sum().item() for c in "uvw"))
     div = compute_divergence(flow32.u, flow32.v, flow32.w, n, n, n, flow32.dx, flow32.dy, flow32.dz_f)
     sl_ms, sl_cnt = phases["sl"]
-    from slchannel_b200 import _native as N
-
     _, flops_alg, pts = sl_algorithmic(n, order)
     t_sl = sl_ms / 1000.0 / max(sl_cnt, 1)
     fp32_peak = N.fma_peak_gflops(False)
@@ -458,6 +461,8 @@ def measure_mixed(flow64, n, order, K, W, dist):
                           "peak_source": "measured on this GPU: slc_fma_peak (FP32 FMA chains, "
                                          "best of 3); the gather's arithmetic is mostly FP32"},
             "phase_ms": {p: v[0] / max(v[1], 1) for p, v in phases.items() if v[1]},
+            "staged_gather": {"blocks": gstats[1], "near_boxes_staged": gstats[2],
+                              "far_boxes_staged": gstats[3], "timeouts": gstats[0]},
             "vs_fp64_after_steps": S, "rel_linf_err_vs_fp64": max(errs), "rel_l2_err_vs_fp64": l2,
             "max_div": float(div.abs().max()),
             "form": "FP32 fluctuation about FP64 plane means in trace+gather; rest FP64"}

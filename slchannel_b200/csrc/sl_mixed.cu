@@ -10,8 +10,10 @@
 // is its 'fp32_accum64' path (semilag.py:249-256, semilag_triton.py), which
 // runs the whole interpolation in FP32 instead.
 #include <algorithm>
+#include <climits>
 
 #include "slc_internal.h"
+#include "slc_tma.cuh"
 
 namespace {
 
@@ -392,6 +394,248 @@ __global__ void __launch_bounds__(kThreads, SLC_SLM_MIN_BLOCKS)
     add_clamps(nclamp, ncl);
 }
 
+// ---- the BDF2 trace+gather with TMA-staged FP32 boxes ------------------------
+// A block is 2 (x) x 4 (y) x 32 (z) arrival points, one warp per 32 z.  Every
+// thread traces both feet (the FP32 trace above); the block takes the min and
+// max of the feet's stencil bases, and where a foot's bounding box fits
+// kMBX x kMBY x kMBZ nodes one thread loads it by TMA (no multicast) from the
+// halo-padded FP32 copy of V^n (near foot) or V^{n-1} (far foot) onto an
+// mbarrier.  A box row is 64 floats = 256 bytes, two whole bank cycles, so a
+// lane whose stencil base moved one row in x or y (the floor of its foot
+// coordinate flipped) keeps its bank.  Blocks whose feet spread wider gather
+// through L1 from the same padded copies.  Weights, the contraction order and
+// the FP64 mean term are gather_foot32's, so the results equal k_sl_mixed's.
+constexpr int kMTI = 2, kMTJ = 4, kMTK = 32;   // arrival tile (x, y, z)
+// staged box (x, y, z) in nodes: 25.6 KB, so the two boxes of a block let
+// four blocks share an SM (at 64 registers), as the L1 kernel runs.  Measured
+// at 256^3 (mixed trace+gather per step): boxes 12 deep in y at three
+// blocks per SM 6.56 ms, 10 deep at three 6.49 ms, 10 deep at four 6.02 ms;
+// two blocks per SM (128 registers, no spill) 7.98 ms.
+#ifndef SLC_SLMT_BOX_Y
+#define SLC_SLMT_BOX_Y 10
+#endif
+constexpr int kMBX = 10, kMBY = SLC_SLMT_BOX_Y, kMBZ = 64;
+constexpr int kMBoxElems = kMBX * kMBY * kMBZ;
+constexpr size_t kMBoxBytes = (size_t)kMBoxElems * sizeof(float);
+constexpr size_t kMSmemBytes = 2 * kMBoxBytes + 1024;  // + alignment slack
+#ifndef SLC_SLMT_MIN_BLOCKS
+#define SLC_SLMT_MIN_BLOCKS 4
+#endif
+static_assert(kMTI * kMTJ * kMTK == kThreads, "one thread per arrival point");
+static_assert((kMBZ * sizeof(float)) % 128 == 0, "box rows of whole bank cycles");
+
+// A foot located for the staged gather: x and y stencil bases (unwrapped,
+// relative to the tile origin), their fractions, the clamped height and the
+// z base; split32's and gather_foot32's arithmetic without the wrap.
+struct FootM32 {
+    double z;
+    float tx, ty;
+    int rx, ry, k0;
+};
+
+template <int C, int O>
+__device__ __forceinline__ FootM32 locate_foot_m32(const SlcParams &P, const Arr32 &A, float ddx, float ddy,
+                                                   float ddz, int i0, int j0, unsigned &ncl)
+{
+    constexpr int h = O / 2 - 1;
+    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
+    if (ddz < A.dzlo || ddz > A.dzhi) ncl += 1;
+    FootM32 F;
+    F.z = A.za + (double)clampdz(A, ddz);
+    const int xi = (C == 0) ? A.xa : A.xb;
+    const float xf = (C == 0) ? A.fxa : A.fxb;
+    const int yi = (C == 1) ? A.ya : A.yb;
+    const float yf = (C == 1) ? A.fya : A.fyb;
+    float fr = fminf(fmaxf(xf + ddx, -1.0e6f), 1.0e6f);
+    float fl = floorf(fr);
+    F.tx = fr - fl;
+    F.rx = xi + (int)fl - h - i0;
+    fr = fminf(fmaxf(yf + ddy, -1.0e6f), 1.0e6f);
+    fl = floorf(fr);
+    F.ty = fr - fl;
+    F.ry = yi + (int)fl - h - j0;
+    const int c = face_cell32(P, (float)F.z);
+    const int m0 = Comp<C>::centers ? c + (F.z >= __ldg(P.zc + c + 1) ? 1 : 0) : c;
+    F.k0 = min(max(m0 - h, 0), NZ - O);
+    return F;
+}
+
+// gather_foot32's weights and contraction over a staged box (ox, oy, oz:
+// the stencil's first node inside the box) plus its FP64 mean term.
+template <int C, int O>
+__device__ __forceinline__ double gather_box_m32(const SlcParams &P, const MixedView &F, const float *box,
+                                                 const FootM32 &f, int ox, int oy, int oz)
+{
+    const int NZ = Comp<C>::centers ? P.nz + 2 : P.nz + 1;
+    float wx[O], wy[O], wz[O];
+    uniform_weights<O, float>(P, f.tx, wx);
+    uniform_weights<O, float>(P, f.ty, wy);
+    {
+        const double *zn = Comp<C>::centers ? P.zc : P.zf;
+        const float *di = (Comp<C>::centers ? P.dinv_c32[O] : P.dinv_f32[O]) + f.k0;
+        float d[O], pre[O];
+#pragma unroll
+        for (int l = 0; l < O; ++l) d[l] = (float)(f.z - __ldg(zn + f.k0 + l));
+        pre[0] = 1.f;
+#pragma unroll
+        for (int l = 1; l < O; ++l) pre[l] = pre[l - 1] * d[l - 1];
+        float suf = 1.f;
+#pragma unroll
+        for (int m = O - 1; m >= 0; --m) {
+            wz[m] = pre[m] * suf * __ldg(di + m * (NZ - O + 1));
+            suf = suf * d[m];
+        }
+    }
+    const float *b = box + (ox * kMBY + oy) * kMBZ + oz;
+    float acc = 0.f;
+#pragma unroll
+    for (int i = 0; i < O; ++i) {
+        float accy = 0.f;
+#pragma unroll
+        for (int j = 0; j < O; ++j) {
+            const float *row = b + (i * kMBY + j) * kMBZ;
+            float accz = 0.f;
+#pragma unroll
+            for (int k = 0; k < O; ++k) accz = fmaf(wz[k], row[k], accz);
+            accy = fmaf(wy[j], accz, accy);
+        }
+        acc = fmaf(wx[i], accy, acc);
+    }
+    double mean = 0.0;
+#pragma unroll
+    for (int k = 0; k < O; ++k) mean = fma((double)wz[k], __ldg(F.mean + f.k0 + k), mean);
+    return (double)acc + mean;
+}
+
+template <int C, int O, int TO>
+__global__ void __launch_bounds__(kThreads, SLC_SLMT_MIN_BLOCKS)
+    k_sl_mixed_tma(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3M M,
+                   const __grid_constant__ MixedView FA, const __grid_constant__ MixedView FB,
+                   const double *__restrict__ fn, const double *__restrict__ fnm1, double dt,
+                   double *__restrict__ out, unsigned long long *nclamp, unsigned long long *stats,
+                   const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB)
+{
+    extern __shared__ unsigned char smraw[];
+    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ int red[12];  // per foot: min/max of rx, ry, k0
+    float *boxA = (float *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    float *boxB = boxA + kMBoxElems;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int i0 = blockIdx.z * kMTI, j0 = blockIdx.y * kMTJ;
+    const int k = blockIdx.x * kMTK + lane;
+    const int j = j0 + ((tid >> 5) & (kMTJ - 1));
+    const int i = i0 + (tid >> 7);
+    const int nzi = (C == 2) ? P.nz - 1 : P.nz;
+    const bool act = k < nzi && j < P.ny && i < P.nx;
+    const unsigned barA = smem_u32(&mbar[0]), barB = smem_u32(&mbar[1]);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            red[2 * q] = INT_MAX;
+            red[2 * q + 1] = INT_MIN;
+        }
+        mbar_init(barA, 1);
+        mbar_init(barB, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    unsigned ncl = 0;
+    Arr32 A{};
+    float ddx = 0.f, ddy = 0.f, ddz = 0.f, fdx = 0.f, fdy = 0.f, fdz = 0.f;
+    FootM32 Fn{}, Fm{};
+    if (act) {
+        A = arrival32<C>(P, i, j, k);
+        float us0, vs0, ws0;
+        if (TO == 4) {
+            sample3_32_o4(P, M, A, 0.f, 0.f, 0.f, us0, vs0, ws0);
+        } else {
+            double u0, v0, w0;
+            arrival_sample<C>(P, M, i, j, k, NodeValMixed32(), u0, v0, w0);
+            us0 = (float)u0;
+            vs0 = (float)v0;
+            ws0 = (float)w0;
+        }
+        trace_foot32<TO>(P, M, A, (float)(0.5 * dt), us0, vs0, ws0, ddx, ddy, ddz);
+        trace_foot32<TO>(P, M, A, (float)dt, us0, vs0, ws0, fdx, fdy, fdz);
+        Fn = locate_foot_m32<C, O>(P, A, ddx, ddy, ddz, i0, j0, ncl);
+        Fm = locate_foot_m32<C, O>(P, A, fdx, fdy, fdz, i0, j0, ncl);
+    }
+    {  // block min/max of the stencil bases: warp reductions, then shared atomics
+        const int v[6] = {Fn.rx, Fn.ry, Fn.k0, Fm.rx, Fm.ry, Fm.k0};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const int lo = __reduce_min_sync(0xffffffffu, act ? v[q] : INT_MAX);
+            const int hi = __reduce_max_sync(0xffffffffu, act ? v[q] : INT_MIN);
+            if (lane == 0) {
+                atomicMin(&red[2 * q], lo);
+                atomicMax(&red[2 * q + 1], hi);
+            }
+        }
+    }
+    __syncthreads();
+    bool fit[2];
+    int X0[2] = {0, 0}, Y0[2] = {0, 0}, Z0[2] = {0, 0};
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        const int *r = red + 6 * f;
+        fit[f] = r[0] <= r[1] && r[1] - r[0] + O <= kMBX && r[3] - r[2] + O <= kMBY &&
+                 r[5] + O - (r[4] & ~3) <= kMBZ;
+        if (fit[f]) {  // the bases are within a few million nodes: no overflow
+            int x0 = (i0 + r[0]) % P.nx;
+            if (x0 < 0) x0 += P.nx;
+            int y0 = (j0 + r[2]) % P.ny;
+            if (y0 < 0) y0 += P.ny;
+            X0[f] = x0;
+            Y0[f] = y0;
+            Z0[f] = r[4] & ~3;  // a multiple of 4 floats: 16-byte aligned inner coordinate
+        }
+    }
+    if (tid == 0) {
+        // stats: [0] time-outs, [1] blocks, [2] near boxes staged, [3] far boxes staged
+        atomicAdd(stats + 1, 1ull);
+        if (fit[0]) atomicAdd(stats + 2, 1ull);
+        if (fit[1]) atomicAdd(stats + 3, 1ull);
+        if (fit[0]) {
+            mbar_expect_tx(barA, (unsigned)kMBoxBytes);
+            tma_load_3d(smem_u32(boxA), &tmA, Z0[0], Y0[0], X0[0], barA);
+        }
+        if (fit[1]) {
+            mbar_expect_tx(barB, (unsigned)kMBoxBytes);
+            tma_load_3d(smem_u32(boxB), &tmB, Z0[1], Y0[1], X0[1], barB);
+        }
+    }
+    if (act) {
+        unsigned none = 0;  // the clamps were counted when the feet were located
+        double ubar, ubb;
+        bool staged = fit[0] && mbar_wait(barA);
+        if (fit[0] && !staged) atomicAdd(stats, 1ull);
+        if (staged)
+            ubar = gather_box_m32<C, O>(P, FA, boxA, Fn, Fn.rx - red[0], Fn.ry - red[2], Fn.k0 - Z0[0]);
+        else
+            ubar = gather_foot32<C, O>(P, FA, A, ddx, ddy, ddz, none);
+        staged = fit[1] && mbar_wait(barB);
+        if (fit[1] && !staged) atomicAdd(stats, 1ull);
+        if (staged)
+            ubb = gather_box_m32<C, O>(P, FB, boxB, Fm, Fm.rx - red[6], Fm.ry - red[8], Fm.k0 - Z0[1]);
+        else
+            ubb = gather_foot32<C, O>(P, FB, A, fdx, fdy, fdz, none);
+        const double Rn = xy_diffusion64<C>(P, fn, i, j, k);
+        const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion64<C>(P, fnm1, i, j, k);
+        double res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
+        res = res + ((2.0 / 3.0) * dt) * Rh;
+        const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
+        out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
+    }
+    add_clamps(nclamp, ncl);
+    // no copy may still be writing this block's shared memory when it exits;
+    // a drain that gives up is counted with the other time-outs
+    if (tid == 0) {
+        if (fit[0] && !mbar_wait(barA)) atomicAdd(stats, 1ull);
+        if (fit[1] && !mbar_wait(barB)) atomicAdd(stats, 1ull);
+    }
+}
+
 // ---- plane means -----------------------------------------------------------
 // Field f of `srcs` (component comp[f], ghost-shaped FP64): block (b, f) sums
 // the b-th of G contiguous ranges of node columns level by level (threads
@@ -509,6 +753,8 @@ struct PackArgs {
     float *f32[9];
     const double *mean[9];
     int nzp[3];
+    float *pad[6];  // non-null: V^n, V^{n-1} go to these halo-padded copies instead
+    int PX, PY;
 };
 
 // One thread per level (blockDim.x >= NZp, or a loop over levels) over kPackJ
@@ -522,6 +768,8 @@ struct PackOne {
     float *fa, *fb, *fm;               // node buffers, NZp levels per column
     const double *ma, *mb, *mm;        // plane means
     int NZp;
+    float *pa = nullptr, *pb = nullptr;  // halo-padded (PX, PY, NZp) copies in place of fa, fb
+    int PX = 0, PY = 0;
 };
 
 __device__ __forceinline__ void pack_mixed(const SlcParams &P, const PackOne &a, int comp, int i,
@@ -550,16 +798,25 @@ __device__ __forceinline__ void pack_mixed(const SlcParams &P, const PackOne &a,
             const int j = jb * kPackJ + q;
             if (j >= P.ny) continue;
             const size_t o = ((size_t)i * P.ny + j) * NZp + k;
-            if (!in) {  // padding levels
-                a.fa[o] = 0.f;
-                a.fb[o] = 0.f;
-                a.fm[o] = 0.f;
-                continue;
+            float fa = 0.f, fb = 0.f, fm = 0.f;  // padding levels stay zero
+            if (in) {
+                const double m = pm ? vm[q] : 2.0 * va[q] - vb[q];
+                fa = (float)(va[q] - ma);
+                fb = (float)(vb[q] - mb);
+                fm = (float)(m - mm);
             }
-            const double m = pm ? vm[q] : 2.0 * va[q] - vb[q];
-            a.fa[o] = (float)(va[q] - ma);
-            a.fb[o] = (float)(vb[q] - mb);
-            a.fm[o] = (float)(m - mm);
+            a.fm[o] = fm;
+            if (a.pa) {  // node (i, j) and its periodic images inside the halo
+                for (int x = i; x < a.PX; x += P.nx)
+                    for (int y = j; y < a.PY; y += P.ny) {
+                        const size_t po = ((size_t)x * a.PY + y) * NZp + k;
+                        a.pa[po] = fa;
+                        a.pb[po] = fb;
+                    }
+            } else {
+                a.fa[o] = fa;
+                a.fb[o] = fb;
+            }
         }
     }
 }
@@ -578,6 +835,12 @@ __global__ void __launch_bounds__(1024) k_pack_mixed(SlcParams P, const __grid_c
     o.mb = a.mean[comp + 3];
     o.mm = a.mean[comp + 6];
     o.NZp = a.nzp[comp];
+    if (a.pad[comp]) {
+        o.pa = a.pad[comp];
+        o.pb = a.pad[comp + 3];
+        o.PX = a.PX;
+        o.PY = a.PY;
+    }
     pack_mixed(P, o, comp, i, blockIdx.x);
 }
 
@@ -721,7 +984,7 @@ int mixed_nzp(int NZ) { return (NZ + 3) & ~3; }
 size_t mixed_partials_doubles(const SlcParams &P) { return (size_t)9 * kMeanBlocks * (P.nz + 2); }
 
 cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const MixedWS &ws,
-                                 cudaStream_t s)
+                                 cudaStream_t s, const TmaMixed *pad)
 {
     MeanSrcs S{};
     const bool explicit_m = M.u != nullptr;
@@ -753,6 +1016,11 @@ cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const 
         a.f32[q] = ws.f32[q];
         a.mean[q] = ws.mean[q];
     }
+    if (pad) {
+        for (int q = 0; q < 6; ++q) a.pad[q] = pad->pad[q];
+        a.PX = pad->PX;
+        a.PY = pad->PY;
+    }
     const int nzp_max = ws.nzp[0] > ws.nzp[2] ? ws.nzp[0] : ws.nzp[2];
     k_pack_mixed<<<dim3((P.ny + kPackJ - 1) / kPackJ, 3 * P.nx), mixed_pack_threads(nzp_max), 0, s>>>(P, a);
     count_launches(3);
@@ -774,6 +1042,88 @@ cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, cons
         else launch_t<6, 2>(P, fn, fnm1, ws, dt, out, nclamp, om, s);
     }
     return cudaGetLastError();
+}
+
+namespace {
+template <int O, int TO>
+cudaError_t launch_mtma_t(const SlcParams &P, const Vel3M &M, const MixedView *FA, const MixedView *FB, Tri fn,
+                          Tri fnm1, double dt, TriMut out, unsigned long long *ncl, unsigned long long *stats,
+                          const CUtensorMap *tm, cudaStream_t s)
+{
+    const dim3 gc((P.nz + kMTK - 1) / kMTK, (P.ny + kMTJ - 1) / kMTJ, (P.nx + kMTI - 1) / kMTI);
+    const dim3 gw((P.nz - 1 + kMTK - 1) / kMTK, (P.ny + kMTJ - 1) / kMTJ, (P.nx + kMTI - 1) / kMTI);
+    // per device context, so set on every launch (a host-side attribute write)
+    cudaError_t e = cudaFuncSetAttribute(k_sl_mixed_tma<0, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kMSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sl_mixed_tma<1, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kMSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sl_mixed_tma<2, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kMSmemBytes);
+    if (e != cudaSuccess) return e;
+    k_sl_mixed_tma<0, O, TO><<<gc, kThreads, kMSmemBytes, s>>>(P, M, FA[0], FB[0], fn.u, fnm1.u, dt, out.u, ncl,
+                                                               stats, tm[0], tm[3]);
+    k_sl_mixed_tma<1, O, TO><<<gc, kThreads, kMSmemBytes, s>>>(P, M, FA[1], FB[1], fn.v, fnm1.v, dt, out.v, ncl,
+                                                               stats, tm[1], tm[4]);
+    if (P.nz > 1)
+        k_sl_mixed_tma<2, O, TO><<<gw, kThreads, kMSmemBytes, s>>>(P, M, FA[2], FB[2], fn.w, fnm1.w, dt, out.w,
+                                                                   ncl, stats, tm[2], tm[5]);
+    count_launches(P.nz > 1 ? 3 : 2);
+    return cudaGetLastError();
+}
+}  // namespace
+
+bool mixed_tma_supported(const SlcParams &P)
+{
+    // every padded row holds a whole box depth (the shallower w rows too)
+    return mixed_nzp(P.nz + 1) >= kMBZ;
+}
+
+size_t mixed_tma_elems(const SlcParams &P, const MixedWS &ws, int comp)
+{
+    return (size_t)(P.nx + kMBX) * (P.ny + kMBY) * ws.nzp[comp];
+}
+
+cudaError_t mixed_tma_encode(const SlcParams &P, const MixedWS &ws, TmaMixed &T)
+{
+    static_assert(sizeof(CUtensorMap) == 128, "tensor-map storage");
+    T.PX = P.nx + kMBX;
+    T.PY = P.ny + kMBY;
+    for (int q = 0; q < 6; ++q) {
+        const unsigned long long nzp = (unsigned long long)ws.nzp[q % 3];
+        const unsigned long long dims[3] = {nzp, (unsigned long long)T.PY, (unsigned long long)T.PX};
+        const unsigned long long strides[2] = {nzp * 4, nzp * 4 * (unsigned long long)T.PY};
+        const unsigned box[3] = {(unsigned)kMBZ, (unsigned)kMBY, (unsigned)kMBX};
+        cudaError_t e = tma_encode_3d(T.maps + 128 * q, true, T.pad[q], dims, strides, box);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_sl_mixed_tma(const SlcParams &P, Tri fn, Tri fnm1, const MixedWS &ws, const TmaMixed &T,
+                                double dt, TriMut out, unsigned long long *nclamp,
+                                unsigned long long *stats, cudaStream_t s)
+{
+    const Vel3M M{mview(ws, 6, P), mview(ws, 7, P), mview(ws, 8, P)};
+    MixedView FA[3], FB[3];
+    for (int c = 0; c < 3; ++c) {
+        for (int w = 0; w < 2; ++w) {
+            MixedView &v = w == 0 ? FA[c] : FB[c];
+            v.f.p = T.pad[c + 3 * w];
+            v.f.sy = ws.nzp[c];
+            v.f.sx = T.PY * ws.nzp[c];
+            v.mean = ws.mean[c + 3 * w];
+            v.mean32 = ws.mean32[c + 3 * w];
+        }
+    }
+    const CUtensorMap *tm = (const CUtensorMap *)T.maps;
+    const bool t4 = P.traj_order == 4;
+    if (P.order == 4)
+        return t4 ? launch_mtma_t<4, 4>(P, M, FA, FB, fn, fnm1, dt, out, nclamp, stats, tm, s)
+                  : launch_mtma_t<4, 2>(P, M, FA, FB, fn, fnm1, dt, out, nclamp, stats, tm, s);
+    return t4 ? launch_mtma_t<6, 4>(P, M, FA, FB, fn, fnm1, dt, out, nclamp, stats, tm, s)
+              : launch_mtma_t<6, 2>(P, M, FA, FB, fn, fnm1, dt, out, nclamp, stats, tm, s);
 }
 
 int mixed_mean_blocks() { return kMeanBlocks; }

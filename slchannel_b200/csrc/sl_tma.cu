@@ -27,6 +27,7 @@
 #include <mutex>
 
 #include "slc_grid.h"
+#include "slc_tma.cuh"
 
 namespace {
 
@@ -43,53 +44,9 @@ constexpr int kBX = 10, kBY = 12, kBZ = 48;
 constexpr int kBoxElems = kBX * kBY * kBZ;
 constexpr size_t kBoxBytes = (size_t)kBoxElems * sizeof(double);
 constexpr size_t kSmemBytes = 2 * kBoxBytes + 1024;  // + alignment slack
-constexpr int kWaitLimit = 1 << 20;                  // bounded mbarrier polls
 
 static_assert(kTI * kTJ * kTK == kThreads, "one thread per arrival point");
 static_assert((kBZ * sizeof(double)) % 16 == 0, "TMA inner box extent");
-
-__device__ __forceinline__ unsigned smem_u32(const void *p)
-{
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-
-// Poll phase 0 of the barrier at most kWaitLimit times; false on time-out.
-__device__ __forceinline__ bool mbar_wait(unsigned bar)
-{
-    for (int it = 0; it < kWaitLimit; ++it) {
-        unsigned done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(0u)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap *tm, int c0, int c1, int c2,
-                                            unsigned bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
-        "l"((unsigned long long)tm), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
-        : "memory");
-}
 
 // Unwrapped stencil base of one coordinate relative to the tile origin
 // (NaN or far-out values give a large sentinel that no box fits).
@@ -434,4 +391,23 @@ cudaError_t launch_sl_tma(const SlcParams &P, Tri fn, Tri fnm1, Tri mid, double 
     M.w = ghost_view<double>(2, mid.w, P.nx, P.ny, P.nz);
     if (P.order == 4) return launch_tma_t<4>(P, M, fn, fnm1, dt, out, nclamp, stats, T, s);
     return launch_tma_t<6>(P, M, fn, fnm1, dt, out, nclamp, stats, T, s);
+}
+
+// One 3-D tiled tensor map (z innermost, no swizzle, zero fill) over a node
+// array: FP32 or FP64 elements, dims (z, y, x), the y and x strides in
+// bytes, and the box (z, y, x) in elements.
+cudaError_t tma_encode_3d(void *map128, bool fp32, const void *base, const unsigned long long dims[3],
+                          const unsigned long long strides[2], const unsigned box[3])
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t d[3] = {dims[0], dims[1], dims[2]};
+    const cuuint64_t st[2] = {strides[0], strides[1]};
+    const cuuint32_t bx[3] = {box[0], box[1], box[2]};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc((CUtensorMap *)map128, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                     3, const_cast<void *>(base), d, st, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }

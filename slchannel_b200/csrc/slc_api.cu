@@ -173,6 +173,34 @@ int ensure_tma(slc_grid *g)
     return SLC_OK;
 }
 
+int ensure_mixed(slc_grid *g);
+
+// Halo-padded FP32 copies and tensor maps of the mixed form's staged gather;
+// state -1 (L1 gather) when the grid is too shallow for a box or the driver
+// lacks the tensor-map entry point.
+int ensure_mixed_tma(slc_grid *g)
+{
+    if (g->tmx_state) return SLC_OK;
+    int rc = ensure_mixed(g);
+    if (rc) return rc;
+    if (!mixed_tma_supported(g->P)) {
+        g->tmx_state = -1;
+        return SLC_OK;
+    }
+    for (int q = 0; q < 6; ++q) {
+        const size_t n = mixed_tma_elems(g->P, g->mws, q % 3);
+        rc = dalloc(g, &g->tmx.pad[q], n, "padded FP32 copy");
+        if (rc) return rc;
+        SLC_CK(cudaMemset(g->tmx.pad[q], 0, n * sizeof(float)), "memset");
+    }
+    if (mixed_tma_encode(g->P, g->mws, g->tmx) != cudaSuccess) {
+        g->tmx_state = -1;
+        return SLC_OK;
+    }
+    g->tmx_state = 1;
+    return SLC_OK;
+}
+
 int ensure_mixed(slc_grid *g)
 {
     if (g->mixed_ready) return SLC_OK;
@@ -253,13 +281,39 @@ int do_apply_bc(slc_grid *g, double *u, double *v, double *w, cudaStream_t s)
     return SLC_OK;
 }
 
+// Which trace+gather: the step's choice, the L1 gather, or the TMA-staged one.
+enum GatherMode { kGatherDefault, kGatherL1, kGatherStaged };
+#ifndef SLC_MIXED_STAGED_DEFAULT  // the mixed step gathers from TMA-staged boxes
+#define SLC_MIXED_STAGED_DEFAULT 1
+#endif
+
 int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *const prev[3],
                          double dt, double *const out[3], int64_t *nclamp, cudaStream_t s,
-                         bool staged = false)
+                         GatherMode mode = kGatherDefault)
 {
     if (g->mixed) {
         int rc = ensure_mixed(g);
         if (rc) return rc;
+        const bool want = mode == kGatherStaged || (mode == kGatherDefault && SLC_MIXED_STAGED_DEFAULT);
+        if (want) {
+            rc = ensure_mixed_tma(g);
+            if (rc) return rc;
+        }
+        if (want && g->tmx_state == 1) {
+            long t = tim_begin(g, SLC_PHASE_MID, s);
+            SLC_CK(launch_mixed_prepare(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
+                                        Tri{nullptr, nullptr, nullptr}, g->mws, s, &g->tmx),
+                   "mixed-form pack (padded)");
+            tim_end(g, t, s);
+            unsigned long long *ncl = counter(g, nclamp);
+            SLC_CK(cudaMemsetAsync(ncl, 0, sizeof(unsigned long long), s), "memset");
+            t = tim_begin(g, SLC_PHASE_SL, s);
+            SLC_CK(launch_sl_mixed_tma(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]}, g->mws,
+                                       g->tmx, dt, TriMut{out[0], out[1], out[2]}, ncl, g->dev_flags, s),
+                   "mixed trace+gather BDF2 (TMA-staged)");
+            tim_end(g, t, s);
+            return SLC_OK;
+        }
         long t = tim_begin(g, SLC_PHASE_MID, s);
         SLC_CK(launch_mixed_prepare(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
                                     Tri{nullptr, nullptr, nullptr}, g->mws, s),
@@ -274,6 +328,7 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
         tim_end(g, t, s);
         return SLC_OK;
     }
+    const bool staged = mode == kGatherStaged;
     int rc = ensure_mid(g);
     if (!rc && staged) rc = ensure_tma(g);
     if (rc) return rc;
@@ -717,7 +772,7 @@ int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *vn, const
     DeviceGuard dg(g->device);
     const double *cur[3] = {un, vn, wn}, *prev[3] = {unm1, vnm1, wnm1};
     double *out[3] = {ou, ov, ow};
-    return do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, S(stream));
+    return do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, S(stream), kGatherL1);
 }
 
 int slc_trace_gather_bdf2_staged(slc_grid *g, const double *un, const double *vn, const double *wn,
@@ -737,7 +792,7 @@ int slc_trace_gather_bdf2_staged(slc_grid *g, const double *un, const double *vn
     SLC_CK(cudaStreamSynchronize(s), "staged gather: synchronise");
     if (g->dev_flags)
         SLC_CK(cudaMemcpy(&before, g->dev_flags, sizeof(before), cudaMemcpyDeviceToHost), "read stats");
-    int rc = do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, s, true);
+    int rc = do_trace_gather_bdf2(g, cur, prev, dt, out, nclamp, s, kGatherStaged);
     if (rc) return rc;
     SLC_CK(cudaStreamSynchronize(s), "staged gather: synchronise");
     if (g->dev_flags)

@@ -42,6 +42,8 @@ struct slc_grid {
     StatsWS *stats = nullptr;
     TmaSL tma{};
     int tma_state = 0;        // 0 not tried, 1 ready, -1 unavailable (L1 gather path)
+    TmaMixed tmx{};           // the mixed form's staged gather (padded FP32 copies, tensor maps)
+    int tmx_state = 0;        // as tma_state
     unsigned long long *dev_flags = nullptr;  // staged-gather statistics (launch_sl_tma)
     size_t ghost_elems[4] = {0, 0, 0, 0};
     cufftHandle fwd = 0, inv = 0;

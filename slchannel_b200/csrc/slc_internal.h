@@ -108,8 +108,11 @@ struct MixedWS {
 int mixed_nzp(int NZ);
 size_t mixed_partials_doubles(const SlcParams &P);
 // Plane means + FP32 packs of A, B and U* (= M when M.u != NULL, else 2A - B).
+// With pad: the V^n and V^{n-1} fluctuations go to pad's halo-padded copies
+// instead of ws.f32[0..5] (struct TmaMixed below).
+struct TmaMixed;
 cudaError_t launch_mixed_prepare(const SlcParams &P, Tri A, Tri B, Tri M, const MixedWS &ws,
-                                 cudaStream_t s);
+                                 cudaStream_t s, const TmaMixed *pad = nullptr);
 // mode 0 one foot of A, 1 BDF1 predictor, 2 BDF2 predictor; fn/fnm1 FP64 fields for R.
 cudaError_t launch_sl_mixed(const SlcParams &P, int mode, Tri fn, Tri fnm1, const MixedWS &ws,
                             double dt, TriMut out, unsigned long long *nclamp, cudaStream_t s,
@@ -193,6 +196,31 @@ cudaError_t launch_mid_pack(const SlcParams &P, Tri cur, Tri prev, TriMut mid, c
 cudaError_t launch_sl_tma(const SlcParams &P, Tri fn, Tri fnm1, Tri mid, double dt, TriMut out,
                           unsigned long long *nclamp, unsigned long long *stats, const TmaSL &T,
                           cudaStream_t s);
+
+// One 3-D tiled tensor map (128 bytes at map128; z innermost, zero fill):
+// FP32 or FP64 elements, dims (z, y, x), y and x strides in bytes, box
+// (z, y, x) in elements.
+cudaError_t tma_encode_3d(void *map128, bool fp32, const void *base, const unsigned long long dims[3],
+                          const unsigned long long strides[2], const unsigned box[3]);
+
+// ---- sl_mixed.cu: the mixed BDF2 trace+gather with TMA-staged FP32 boxes -------
+// Halo-padded FP32 fluctuation copies of V^n (slots 0-2) and V^{n-1} (3-5):
+// (nx + PX_HALO, ny + PY_HALO, nzp[comp]) with node (i, j) also at
+// (i + nx, j), (i, j + ny) and (i + nx, j + ny) where those fall inside,
+// written by launch_mixed_prepare when it is given this workspace, and their
+// tensor maps.
+struct TmaMixed {
+    float *pad[6];
+    int PX, PY;
+    alignas(64) unsigned char maps[6 * 128];
+};
+bool mixed_tma_supported(const SlcParams &P);
+size_t mixed_tma_elems(const SlcParams &P, const MixedWS &ws, int comp);
+cudaError_t mixed_tma_encode(const SlcParams &P, const MixedWS &ws, TmaMixed &T);
+// stats as launch_sl_tma's
+cudaError_t launch_sl_mixed_tma(const SlcParams &P, Tri fn, Tri fnm1, const MixedWS &ws, const TmaMixed &T,
+                                double dt, TriMut out, unsigned long long *nclamp,
+                                unsigned long long *stats, cudaStream_t s);
 
 // sl_mixed.cu, ensemble forms of the mixed predictor: plane means of V^n and
 // V^{n-1} (items (inst, column group, field 0..5)), their finish, the FP32
