@@ -140,7 +140,9 @@ SLC_API int slc_advect_extra(slc_grid *g, const double *fu, const double *fv, co
  * there, and u_hat = 4/3 ubar - 1/3 ubarbar + (2/3) dt (2 R^n - R^{n-1})
  * written to the interiors of (ou, ov, ow), R the explicit x,y diffusion.
  * cur/prev/out are ghost-shaped; cur and prev must be BC-consistent.
- * *nclamp (device int64) receives the clamp count over both feet.
+ * *nclamp (device int64) receives the clamp count over both feet.  This
+ * entry point gathers through L1 in both precisions (slc_step_bdf2 on a
+ * mixed handle gathers from TMA-staged boxes, the results being equal).
  * Replaces solver.py:846-903 (the two SLAdvector.advect calls and the
  * BDF2 combination). */
 SLC_API int slc_trace_gather_bdf2(slc_grid *g, const double *un, const double *vn, const double *wn,
@@ -185,12 +187,14 @@ SLC_API int slc_host_step_stats(slc_grid *g, int64_t *out4);
 
 /* slc_trace_gather_bdf2 with each block's two gather source boxes staged
  * in shared memory by the Tensor Memory Accelerator (3-D cp.async.bulk.tensor
- * loads of halo-padded node copies written with U*; FP64 handles with
- * nz >= 47, otherwise identical to slc_trace_gather_bdf2).  Results are
- * bit-identical to slc_trace_gather_bdf2.  Not the step's default: its
- * kernel is faster than the L1 one, but at the 256^3 benchmark the extra
- * pass that writes the padded copies takes back the gain; where the feet
- * spread (trajectory CFL 3) the call is the faster of the two.
+ * loads of halo-padded node copies; otherwise identical to
+ * slc_trace_gather_bdf2).  Results are bit-identical to
+ * slc_trace_gather_bdf2's.  FP64 handles (nz >= 47): the padded copies are
+ * written with U*; not the FP64 step's default, since at the 256^3
+ * benchmark that extra pass takes back the kernel's gain, while where the
+ * feet spread (trajectory CFL 3) this call is the faster of the two.  Mixed
+ * handles (nz >= 62): FP32 fluctuation boxes, the padded copies written by
+ * the mixed pack itself; slc_step_bdf2 on a mixed handle gathers this way.
  * slc_gather_stats reports how many boxes were staged.  Synchronous: it
  * waits for `stream` and returns SLC_E_CUDA if any bulk copy of this call
  * did not complete within the kernel's bounded waits (the affected blocks
