@@ -264,10 +264,10 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic_per_point():
-    """DRAM bytes per arrival point of the fused trace+gather kernel, from the
-    ncu summary committed in profiles/ (line 'dram_bytes_per_point: X')."""
-    path = os.path.join(REPO, "profiles", "k_sl_bdf2_o6_fp64.txt")
+def profiled_traffic_per_point(profile="k_sl_bdf2_o6_fp64.txt"):
+    """DRAM bytes per arrival point of a trace+gather kernel, from its ncu
+    summary committed in profiles/ (line 'dram_bytes_per_point: X')."""
+    path = os.path.join(REPO, "profiles", profile)
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_point:"):
@@ -839,6 +839,8 @@ def run_b200(args):
     torch.cuda.synchronize()
 
     flow._grid.timing(True)
+    gstats = (ctypes.c_int64 * 4)()
+    N.check(N.lib().slc_gather_stats(flow._grid.handle, gstats, 1), flow._grid.handle)
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sampler = ClockSampler(gpu_smi_id(dev))
@@ -859,6 +861,9 @@ def run_b200(args):
     ms = ev0.elapsed_time(ev1)
     phases = flow._grid.timing_read()
     flow._grid.timing(False)
+    N.check(N.lib().slc_gather_stats(flow._grid.handle, gstats, 1), flow._grid.handle)
+    staged_gather = {"blocks": gstats[1], "near_boxes_staged": gstats[2], "far_boxes_staged": gstats[3],
+                     "timeouts": gstats[0]}
     ms_max = ms
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -878,12 +883,16 @@ def run_b200(args):
     bytes_alg, flops_alg, pts = sl_algorithmic(n, order)
     peak, peak_kind = measured_peaks()
     achieved = bytes_alg / t_sl / 1e9
-    tpp = profiled_traffic_per_point()
+    staged = staged_gather["blocks"] > 0
+    tpp = profiled_traffic_per_point("k_sl_tma_staged_gather_o6_fp64_128cubed.txt" if staged
+                                     else "k_sl_bdf2_o6_fp64.txt")
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "traffic": (tpp * pts) if tpp else None,
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-        "kernel": f"k_sl<C,{order},BDF2> x3 launches per step (one per velocity component)",
+        "kernel": (f"k_sl_tma<C,{order}> (gather from TMA-staged boxes)" if staged else f"k_sl<C,{order},BDF2>")
+                  + " x3 launches per step (one per velocity component)",
+        "staged_gather": staged_gather,
         "algorithmic_bytes_per_step": bytes_alg,
         "kernel_ms_per_step": t_sl * 1000.0,
         "fp64_gflops": flops_alg / t_sl / 1e9,

@@ -417,7 +417,7 @@ constexpr int kMTI = 2, kMTJ = 4, kMTK = 32;   // arrival tile (x, y, z)
 constexpr int kMBX = 10, kMBY = SLC_SLMT_BOX_Y, kMBZ = 64;
 constexpr int kMBoxElems = kMBX * kMBY * kMBZ;
 constexpr size_t kMBoxBytes = (size_t)kMBoxElems * sizeof(float);
-constexpr size_t kMSmemBytes = 2 * kMBoxBytes + 1024;  // + alignment slack
+constexpr size_t kMSmemBytes = 2 * kMBoxBytes + 128;  // + alignment slack (boxes start on 128 bytes)
 #ifndef SLC_SLMT_MIN_BLOCKS
 #define SLC_SLMT_MIN_BLOCKS 4
 #endif
@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kThreads, SLC_SLMT_MIN_BLOCKS)
     extern __shared__ unsigned char smraw[];
     __shared__ __align__(8) unsigned long long mbar[2];
     __shared__ int red[12];  // per foot: min/max of rx, ry, k0
-    float *boxA = (float *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    float *boxA = (float *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
     float *boxB = boxA + kMBoxElems;
     const int tid = threadIdx.x, lane = tid & 31;
     const int i0 = blockIdx.z * kMTI, j0 = blockIdx.y * kMTJ;

@@ -40,10 +40,23 @@ constexpr int kTI = 2, kTJ = 4, kTK = 32;    // arrival tile (x, y, z)
 // memory: 48 doubles = 384 bytes, a multiple of the 128-byte bank cycle, so
 // lanes whose stencil base moved one row in x or y keep their banks
 // (40 doubles gave 3.12 wavefronts per 8-byte load, 48 gives 2.33)
-constexpr int kBX = 10, kBY = 12, kBZ = 48;
+// x and y extents: 9 x 10 x 48 doubles = 34.6 KB, so the two boxes of a
+// block let three blocks share an SM (80 registers, some spill).  Measured
+// at 256^3 (trace+gather per step, order 6): 10 x 12 boxes at two blocks per
+// SM 10.64 ms, 9 x 10 at three 9.86 ms, the L1 gather 10.73 ms.
+#ifndef SLC_TMA_BOX_X
+#define SLC_TMA_BOX_X 9
+#endif
+#ifndef SLC_TMA_BOX_Y
+#define SLC_TMA_BOX_Y 10
+#endif
+#ifndef SLC_TMA_MIN_BLOCKS
+#define SLC_TMA_MIN_BLOCKS 3
+#endif
+constexpr int kBX = SLC_TMA_BOX_X, kBY = SLC_TMA_BOX_Y, kBZ = 48;
 constexpr int kBoxElems = kBX * kBY * kBZ;
 constexpr size_t kBoxBytes = (size_t)kBoxElems * sizeof(double);
-constexpr size_t kSmemBytes = 2 * kBoxBytes + 1024;  // + alignment slack
+constexpr size_t kSmemBytes = 2 * kBoxBytes + 128;  // + alignment slack (boxes start on 128 bytes)
 
 static_assert(kTI * kTJ * kTK == kThreads, "one thread per arrival point");
 static_assert((kBZ * sizeof(double)) % 16 == 0, "TMA inner box extent");
@@ -126,7 +139,7 @@ __device__ __forceinline__ double gather_global(const SlcParams &P, NodeView<dou
 }
 
 template <int C, int O>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, SLC_TMA_MIN_BLOCKS)
     k_sl_tma(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, const double *__restrict__ fn, const double *__restrict__ fnm1,
              double dt, double *__restrict__ out, unsigned long long *nclamp, unsigned long long *stats,
              const __grid_constant__ CUtensorMap tmN, const __grid_constant__ CUtensorMap tmM)
@@ -134,7 +147,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     extern __shared__ unsigned char smraw[];
     __shared__ __align__(8) unsigned long long mbar[2];
     __shared__ int red[12];  // per foot: min/max of rx, ry, k0
-    double *boxN = (double *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    double *boxN = (double *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
     double *boxM = boxN + kBoxElems;
     const int tid = threadIdx.x;
     const int i0 = blockIdx.z * kTI, j0 = blockIdx.y * kTJ;

@@ -2,6 +2,7 @@
 // entry points that sequence the kernels of the SL-BDF2 step on a stream.
 #include <cufft.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -286,6 +287,69 @@ enum GatherMode { kGatherDefault, kGatherL1, kGatherStaged };
 #ifndef SLC_MIXED_STAGED_DEFAULT  // the mixed step gathers from TMA-staged boxes
 #define SLC_MIXED_STAGED_DEFAULT 1
 #endif
+#ifndef SLC_FP64_STAGED_DEFAULT  // so does the FP64 step at order 6
+#define SLC_FP64_STAGED_DEFAULT 1
+#endif
+// The step keeps gathering from staged boxes while at least this fraction of
+// the blocks staged both feet, and otherwise gathers through L1 (whose
+// kernel holds more registers per thread, so it is the faster when many
+// blocks would fall back), trying the staged gather again every
+// kStagedProbeEvery calls.  The two gathers give the same results.
+constexpr double kStagedMinFraction = 0.9;
+constexpr int kStagedProbeEvery = 50;
+
+bool capturing(cudaStream_t s)
+{
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone;
+}
+
+// The default mode's choice, from the staged-box counters of an earlier call
+// (copied to pinned host memory behind that call, read here once its event
+// has completed: no synchronisation).
+bool choose_staged(slc_grid *g, cudaStream_t s)
+{
+    GatherChoice &c = g->gchoice;
+    if (capturing(s)) return c.staged;  // no bookkeeping inside a graph capture
+    if (c.pending) {
+        const cudaError_t q = cudaEventQuery(c.ev);
+        if (q == cudaSuccess) {
+            const unsigned long long *h = c.host;
+            auto delta = [&](int k) { return h[k] >= c.last[k] ? h[k] - c.last[k] : h[k]; };  // reset between
+            const unsigned long long blocks = delta(1), both = std::min(delta(2), delta(3));
+            if (blocks > 0) c.staged = (double)both >= kStagedMinFraction * (double)blocks;
+            for (int k = 0; k < 4; ++k) c.last[k] = h[k];
+            c.pending = false;
+        } else if (q == cudaErrorNotReady && cudaPeekAtLastError() == cudaErrorNotReady) {
+            cudaGetLastError();  // "not ready" is no error of the caller's
+        }
+    }
+    if (!c.staged && ++c.calls_l1 >= kStagedProbeEvery) {
+        c.calls_l1 = 0;
+        return true;  // probe: the counters of this call decide again
+    }
+    return c.staged;
+}
+
+// After a staged launch of the default mode: copy the counters behind it.
+void note_staged(slc_grid *g, cudaStream_t s)
+{
+    GatherChoice &c = g->gchoice;
+    if (c.pending || capturing(s)) return;
+    if (!c.host) {
+        void *h = nullptr;
+        if (cudaHostAlloc(&h, 4 * sizeof(unsigned long long), cudaHostAllocDefault) != cudaSuccess) return;
+        if (cudaEventCreateWithFlags(&c.ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaFreeHost(h);
+            return;
+        }
+        c.host = (unsigned long long *)h;
+    }
+    if (cudaMemcpyAsync(c.host, g->dev_flags, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) ==
+            cudaSuccess &&
+        cudaEventRecord(c.ev, s) == cudaSuccess)
+        c.pending = true;
+}
 
 int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *const prev[3],
                          double dt, double *const out[3], int64_t *nclamp, cudaStream_t s,
@@ -294,10 +358,14 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
     if (g->mixed) {
         int rc = ensure_mixed(g);
         if (rc) return rc;
-        const bool want = mode == kGatherStaged || (mode == kGatherDefault && SLC_MIXED_STAGED_DEFAULT);
+        // at order 4 the mixed step keeps its L1 gather (5.37 against 5.80 ms
+        // per tricubic step at 256^3)
+        bool want = mode == kGatherStaged ||
+                    (mode == kGatherDefault && SLC_MIXED_STAGED_DEFAULT && g->P.order == 6);
         if (want) {
             rc = ensure_mixed_tma(g);
             if (rc) return rc;
+            if (mode == kGatherDefault && g->tmx_state == 1) want = choose_staged(g, s);
         }
         if (want && g->tmx_state == 1) {
             long t = tim_begin(g, SLC_PHASE_MID, s);
@@ -312,6 +380,7 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
                                        g->tmx, dt, TriMut{out[0], out[1], out[2]}, ncl, g->dev_flags, s),
                    "mixed trace+gather BDF2 (TMA-staged)");
             tim_end(g, t, s);
+            if (mode == kGatherDefault) note_staged(g, s);
             return SLC_OK;
         }
         long t = tim_begin(g, SLC_PHASE_MID, s);
@@ -328,10 +397,14 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
         tim_end(g, t, s);
         return SLC_OK;
     }
-    const bool staged = mode == kGatherStaged;
+    // the FP64 staged kernel holds three blocks per SM; at order 4 the L1
+    // kernel runs four and stays the faster
+    bool staged = mode == kGatherStaged ||
+                  (mode == kGatherDefault && SLC_FP64_STAGED_DEFAULT && g->P.order == 6);
     int rc = ensure_mid(g);
     if (!rc && staged) rc = ensure_tma(g);
     if (rc) return rc;
+    if (staged && mode == kGatherDefault && g->tma_state == 1) staged = choose_staged(g, s);
     if (staged && g->tma_state == 1) {
         long t = tim_begin(g, SLC_PHASE_MID, s);
         SLC_CK(launch_mid_pack(g->P, Tri{cur[0], cur[1], cur[2]}, Tri{prev[0], prev[1], prev[2]},
@@ -346,6 +419,7 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
                              ncl, g->dev_flags, g->tma, s),
                "trace+gather BDF2 (TMA-staged)");
         tim_end(g, t, s);
+        if (mode == kGatherDefault) note_staged(g, s);
         return SLC_OK;
     }
     long t = tim_begin(g, SLC_PHASE_MID, s);
@@ -597,6 +671,11 @@ int slc_grid_destroy(slc_grid *g)
         cudaDeviceSynchronize();  // copies in flight may still use the host buffers
         host_step_free(g->host);
     }
+    if (g->gchoice.host) {
+        cudaDeviceSynchronize();  // a counter copy may still be in flight
+        cudaFreeHost(g->gchoice.host);
+    }
+    if (g->gchoice.ev) cudaEventDestroy(g->gchoice.ev);
     delete g;
     return SLC_OK;
 }

@@ -17,6 +17,17 @@ void host_step_free(HostStep *h);
 struct StatsWS;               // diagnostics / statistics workspace (diagnostics.cu), on first use
 void stats_free(StatsWS *s);
 
+// The step's choice between the TMA-staged and the L1 gather (slc_api.cu),
+// from the staged-box counters of earlier calls, read back asynchronously.
+struct GatherChoice {
+    bool staged = true;
+    bool pending = false;                // a counter copy is in flight behind ev
+    unsigned long long *host = nullptr;  // pinned copy of dev_flags
+    cudaEvent_t ev = nullptr;
+    unsigned long long last[4] = {0, 0, 0, 0};
+    int calls_l1 = 0;
+};
+
 struct slc_grid {
     SlcParams P{};
     int device = 0;
@@ -45,6 +56,7 @@ struct slc_grid {
     TmaMixed tmx{};           // the mixed form's staged gather (padded FP32 copies, tensor maps)
     int tmx_state = 0;        // as tma_state
     unsigned long long *dev_flags = nullptr;  // staged-gather statistics (launch_sl_tma)
+    GatherChoice gchoice;
     size_t ghost_elems[4] = {0, 0, 0, 0};
     cufftHandle fwd = 0, inv = 0;
     bool plans = false;
