@@ -7,13 +7,13 @@
 // 128-byte lines at most alignments) and from shared memory two when its
 // lanes read one row of the box.  The kernel is bound by that data pipe.
 // Lanes whose foot coordinate floors to the next row in x or y read another
-// row; the box depth keeps such lanes on their banks (kBZ below).
+// row; the box depth keeps such lanes on their banks (Box below).
 //
 // How: a block is a tile of 2 (x) x 4 (y) x 32 (z) arrival points, one warp
 // per 32 z.  Every thread traces both feet (the iterated midpoint rule of
 // sl_device.cuh, unchanged).  Shared-memory integer min/max of the feet's
 // stencil bases give each foot's bounding box.  If it fits the fixed box of
-// kBX x kBY x kBZ nodes, one thread issues a 3-D cp.async.bulk.tensor load of
+// the order's box (Box<O>), one thread issues a 3-D cp.async.bulk.tensor load of
 // the box (no multicast) from a halo-padded node copy of V^n (near foot) or
 // V^{n-1} (far foot) onto an mbarrier, and the threads gather from shared
 // memory.  A block whose feet spread wider uses the L1 gather.  The boxes
@@ -40,10 +40,15 @@ constexpr int kTI = 2, kTJ = 4, kTK = 32;    // arrival tile (x, y, z)
 // memory: 48 doubles = 384 bytes, a multiple of the 128-byte bank cycle, so
 // lanes whose stencil base moved one row in x or y keep their banks
 // (40 doubles gave 3.12 wavefronts per 8-byte load, 48 gives 2.33)
-// x and y extents: 9 x 10 x 48 doubles = 34.6 KB, so the two boxes of a
-// block let three blocks share an SM (80 registers, some spill).  Measured
-// at 256^3 (trace+gather per step, order 6): 10 x 12 boxes at two blocks per
-// SM 10.64 ms, 9 x 10 at three 9.86 ms, the L1 gather 10.73 ms.
+// Staged box (x, y, z) in nodes and resident blocks per SM, per order.  The
+// z extent sets the row stride in shared memory: 48 doubles = 384 bytes, a
+// multiple of the 128-byte bank cycle, so lanes whose stencil base moved one
+// row in x or y keep their banks (40 doubles gave 3.12 wavefronts per 8-byte
+// load, 48 gives 2.33).  Order 6: 9 x 10 x 48 doubles = 34.6 KB, so the two
+// boxes of a block let three blocks share an SM (80 registers, some spill);
+// measured at 256^3 (trace+gather per step): 10 x 12 boxes at two blocks per
+// SM 10.64 ms, 9 x 10 at three 9.86 ms, the L1 gather 10.73 ms.  Order 4:
+// 7 x 9 x 48 (24.2 KB) at four blocks per SM, as the L1 kernel runs.
 #ifndef SLC_TMA_BOX_X
 #define SLC_TMA_BOX_X 9
 #endif
@@ -53,12 +58,23 @@ constexpr int kTI = 2, kTJ = 4, kTK = 32;    // arrival tile (x, y, z)
 #ifndef SLC_TMA_MIN_BLOCKS
 #define SLC_TMA_MIN_BLOCKS 3
 #endif
-constexpr int kBX = SLC_TMA_BOX_X, kBY = SLC_TMA_BOX_Y, kBZ = 48;
-constexpr int kBoxElems = kBX * kBY * kBZ;
-constexpr size_t kBoxBytes = (size_t)kBoxElems * sizeof(double);
-constexpr size_t kSmemBytes = 2 * kBoxBytes + 128;  // + alignment slack (boxes start on 128 bytes)
-
-static_assert(kTI * kTJ * kTK == kThreads, "one thread per arrival point");
+#ifndef SLC_TMA_O4_MIN_BLOCKS
+#define SLC_TMA_O4_MIN_BLOCKS 4
+#endif
+template <int O>
+struct Box {
+    static constexpr int X = O == 4 ? 7 : SLC_TMA_BOX_X;
+    static constexpr int Y = O == 4 ? 9 : SLC_TMA_BOX_Y;
+    static constexpr int Z = 48;
+    static constexpr int elems = X * Y * Z;
+    static constexpr size_t bytes = (size_t)elems * sizeof(double);
+    static constexpr size_t smem = 2 * bytes + 128;  // + alignment slack (boxes start on 128 bytes)
+    static constexpr int min_blocks = O == 4 ? SLC_TMA_O4_MIN_BLOCKS : SLC_TMA_MIN_BLOCKS;
+};
+// the padded copies' halo: the largest box
+constexpr int kBX = Box<6>::X > Box<4>::X ? Box<6>::X : Box<4>::X;
+constexpr int kBY = Box<6>::Y > Box<4>::Y ? Box<6>::Y : Box<4>::Y;
+constexpr int kBZ = 48;
 static_assert((kBZ * sizeof(double)) % 16 == 0, "TMA inner box extent");
 
 // Unwrapped stencil base of one coordinate relative to the tile origin
@@ -110,14 +126,14 @@ __device__ __forceinline__ double gather_box(const SlcParams &P, const double *b
     const double *zn = Comp<C>::centers ? P.zc : P.zf;
     const double *dinv = Comp<C>::centers ? P.dinv_c[O] : P.dinv_f[O];
     z_weights<O, double>(zn, dinv, denom_rows(Comp<C>::centers, P.nz, O), F.k0, F.z, wz);
-    const double *b = box + (ox * kBY + oy) * kBZ + oz;
+    const double *b = box + (ox * Box<O>::Y + oy) * Box<O>::Z + oz;
     double acc = 0.0;
 #pragma unroll
     for (int i = 0; i < O; ++i) {
         double accy = 0.0;
 #pragma unroll
         for (int j = 0; j < O; ++j) {
-            const double *row = b + (i * kBY + j) * kBZ;
+            const double *row = b + (i * Box<O>::Y + j) * Box<O>::Z;
             double accz = 0.0;
 #pragma unroll
             for (int k = 0; k < O; ++k) accz = fma(wz[k], row[k], accz);
@@ -139,7 +155,7 @@ __device__ __forceinline__ double gather_global(const SlcParams &P, NodeView<dou
 }
 
 template <int C, int O>
-__global__ void __launch_bounds__(kThreads, SLC_TMA_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, Box<O>::min_blocks)
     k_sl_tma(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, const double *__restrict__ fn, const double *__restrict__ fnm1,
              double dt, double *__restrict__ out, unsigned long long *nclamp, unsigned long long *stats,
              const __grid_constant__ CUtensorMap tmN, const __grid_constant__ CUtensorMap tmM)
@@ -148,7 +164,7 @@ __global__ void __launch_bounds__(kThreads, SLC_TMA_MIN_BLOCKS)
     __shared__ __align__(8) unsigned long long mbar[2];
     __shared__ int red[12];  // per foot: min/max of rx, ry, k0
     double *boxN = (double *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
-    double *boxM = boxN + kBoxElems;
+    double *boxM = boxN + Box<O>::elems;
     const int tid = threadIdx.x;
     const int i0 = blockIdx.z * kTI, j0 = blockIdx.y * kTJ;
     const int k = blockIdx.x * kTK + (tid & 31);
@@ -200,8 +216,8 @@ __global__ void __launch_bounds__(kThreads, SLC_TMA_MIN_BLOCKS)
 #pragma unroll
     for (int f = 0; f < 2; ++f) {
         const int *r = red + 6 * f;
-        fit[f] = r[0] <= r[1] && r[1] - r[0] + O <= kBX && r[3] - r[2] + O <= kBY &&
-                 r[5] + O - (r[4] & ~1) <= kBZ;
+        fit[f] = r[0] <= r[1] && r[1] - r[0] + O <= Box<O>::X && r[3] - r[2] + O <= Box<O>::Y &&
+                 r[5] + O - (r[4] & ~1) <= Box<O>::Z;
         if (fit[f]) {  // r[0], r[2] are small here (|.| < 4096)
             int x0 = (i0 + r[0]) % P.nx;
             if (x0 < 0) x0 += P.nx;
@@ -218,11 +234,11 @@ __global__ void __launch_bounds__(kThreads, SLC_TMA_MIN_BLOCKS)
         if (fit[0]) atomicAdd(stats + 2, 1ull);
         if (fit[1]) atomicAdd(stats + 3, 1ull);
         if (fit[0]) {
-            mbar_expect_tx(barN, (unsigned)kBoxBytes);
+            mbar_expect_tx(barN, (unsigned)Box<O>::bytes);
             tma_load_3d(smem_u32(boxN), &tmN, Z0[0], Y0[0], X0[0], barN);
         }
         if (fit[1]) {
-            mbar_expect_tx(barM, (unsigned)kBoxBytes);
+            mbar_expect_tx(barM, (unsigned)Box<O>::bytes);
             tma_load_3d(smem_u32(boxM), &tmM, Z0[1], Y0[1], X0[1], barM);
         }
     }
@@ -323,17 +339,17 @@ cudaError_t launch_tma_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, do
     const dim3 gc((P.nz + kTK - 1) / kTK, (P.ny + kTJ - 1) / kTJ, (P.nx + kTI - 1) / kTI);
     const dim3 gw((P.nz - 1 + kTK - 1) / kTK, (P.ny + kTJ - 1) / kTJ, (P.nx + kTI - 1) / kTI);
     // per device context, so set on every launch (a host-side attribute write)
-    cudaError_t attr = cudaFuncSetAttribute(k_sl_tma<0, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    cudaError_t attr = cudaFuncSetAttribute(k_sl_tma<0, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
     if (attr == cudaSuccess)
-        attr = cudaFuncSetAttribute(k_sl_tma<1, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+        attr = cudaFuncSetAttribute(k_sl_tma<1, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
     if (attr == cudaSuccess)
-        attr = cudaFuncSetAttribute(k_sl_tma<2, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+        attr = cudaFuncSetAttribute(k_sl_tma<2, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
     if (attr != cudaSuccess) return attr;
     const CUtensorMap *tm = (const CUtensorMap *)T.maps;
-    k_sl_tma<0, O><<<gc, kThreads, kSmemBytes, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl, stats, tm[0], tm[3]);
-    k_sl_tma<1, O><<<gc, kThreads, kSmemBytes, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl, stats, tm[1], tm[4]);
+    k_sl_tma<0, O><<<gc, kThreads, Box<O>::smem, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl, stats, tm[0], tm[3]);
+    k_sl_tma<1, O><<<gc, kThreads, Box<O>::smem, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl, stats, tm[1], tm[4]);
     if (P.nz > 1)
-        k_sl_tma<2, O><<<gw, kThreads, kSmemBytes, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl, stats, tm[2], tm[5]);
+        k_sl_tma<2, O><<<gw, kThreads, Box<O>::smem, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl, stats, tm[2], tm[5]);
     count_launches(P.nz > 1 ? 3 : 2);
     return cudaGetLastError();
 }
@@ -364,7 +380,9 @@ cudaError_t tma_encode(const SlcParams &P, TmaSL &T)
         const cuuint64_t nzp = (cuuint64_t)tma_padded_nz(NZ);
         const cuuint64_t dims[3] = {nzp, (cuuint64_t)(P.ny + kBY), (cuuint64_t)(P.nx + kBX)};
         const cuuint64_t strides[2] = {nzp * 8, nzp * 8 * (cuuint64_t)(P.ny + kBY)};
-        const cuuint32_t box[3] = {(cuuint32_t)kBZ, (cuuint32_t)kBY, (cuuint32_t)kBX};
+        const bool o4 = P.order == 4;
+        const cuuint32_t box[3] = {(cuuint32_t)kBZ, (cuuint32_t)(o4 ? Box<4>::Y : Box<6>::Y),
+                                   (cuuint32_t)(o4 ? Box<4>::X : Box<6>::X)};
         const cuuint32_t estr[3] = {1, 1, 1};
         CUresult r = enc(&tm[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)T.pad[q], dims, strides, box,
                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

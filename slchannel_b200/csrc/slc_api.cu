@@ -290,6 +290,9 @@ enum GatherMode { kGatherDefault, kGatherL1, kGatherStaged };
 #ifndef SLC_FP64_STAGED_DEFAULT  // so does the FP64 step at order 6
 #define SLC_FP64_STAGED_DEFAULT 1
 #endif
+#ifndef SLC_FP64_O4_STAGED_DEFAULT  // and at order 4
+#define SLC_FP64_O4_STAGED_DEFAULT 0
+#endif
 // The step keeps gathering from staged boxes while at least this fraction of
 // the blocks staged both feet, and otherwise gathers through L1 (whose
 // kernel holds more registers per thread, so it is the faster when many
@@ -400,7 +403,7 @@ int do_trace_gather_bdf2(slc_grid *g, const double *const cur[3], const double *
     // the FP64 staged kernel holds three blocks per SM; at order 4 the L1
     // kernel runs four and stays the faster
     bool staged = mode == kGatherStaged ||
-                  (mode == kGatherDefault && SLC_FP64_STAGED_DEFAULT && g->P.order == 6);
+                  (mode == kGatherDefault && (g->P.order == 6 ? SLC_FP64_STAGED_DEFAULT : SLC_FP64_O4_STAGED_DEFAULT));
     int rc = ensure_mid(g);
     if (!rc && staged) rc = ensure_tma(g);
     if (rc) return rc;

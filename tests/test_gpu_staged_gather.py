@@ -3,11 +3,11 @@ by TMA) against slc_trace_gather_bdf2 (gather through L1): equal clamp counts
 and bit-identical outputs, with every box staged (small dt), with many blocks
 falling back to L1 (wide feet), and on a grid too shallow for a box.
 
-At order 4 the L1 kernel is compiled for four resident blocks per SM (64
-registers) and the staged one for two (its boxes take 92 KB of shared memory
-per block), so ptxas may fuse the shared trajectory arithmetic's multiplies
-and adds into FMAs differently in the two: there the outputs agree to
-round-off (<= 1e-13 relative), not bit for bit."""
+At order 4 the two kernels are compiled separately with different spill
+patterns (the staged one holds its boxes' state across the barrier), so
+ptxas may fuse the shared trajectory arithmetic's multiplies and adds into
+FMAs differently: there the outputs agree to round-off (<= 1e-13 relative),
+not bit for bit."""
 
 import ctypes
 import math
