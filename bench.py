@@ -890,7 +890,8 @@ def run_b200(args):
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "traffic": (tpp * pts) if tpp else None,
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-        "kernel": (f"k_sl_tma<C,{order}> (gather from TMA-staged boxes)" if staged else f"k_sl<C,{order},BDF2>")
+        "kernel": (f"k_sl_tma_seq<C,{order}> (gather from TMA-staged boxes, one foot after the other)"
+                   if staged else f"k_sl<C,{order},BDF2>")
                   + " x3 launches per step (one per velocity component)",
         "staged_gather": staged_gather,
         "algorithmic_bytes_per_step": bytes_alg,

@@ -10,13 +10,15 @@
 // row; the box depth keeps such lanes on their banks (Box below).
 //
 // How: a block is a tile of 2 (x) x 4 (y) x 32 (z) arrival points, one warp
-// per 32 z.  Every thread traces both feet (the iterated midpoint rule of
-// sl_device.cuh, unchanged).  Shared-memory integer min/max of the feet's
-// stencil bases give each foot's bounding box.  If it fits the fixed box of
-// the order's box (Box<O>), one thread issues a 3-D cp.async.bulk.tensor load of
-// the box (no multicast) from a halo-padded node copy of V^n (near foot) or
-// V^{n-1} (far foot) onto an mbarrier, and the threads gather from shared
-// memory.  A block whose feet spread wider uses the L1 gather.  The boxes
+// per 32 z.  Every thread traces its feet (the iterated midpoint rule of
+// sl_device.cuh, unchanged).  Warp reductions and shared-memory integer
+// min/max of the feet's stencil bases give each foot's bounding box.  If it
+// fits the order's box (Box<O>), one thread issues a 3-D cp.async.bulk.tensor
+// load of the box (no multicast) from a halo-padded node copy of V^n (near
+// foot) or V^{n-1} (far foot) onto an mbarrier, and the threads gather from
+// shared memory.  A block whose feet spread wider uses the L1 gather.  At
+// order 6 the feet go one after the other through one box buffer
+// (k_sl_tma_seq); at order 4 both boxes are staged at once (k_sl_tma).  The boxes
 // come from padded node copies, written together with U* by k_mid_pack:
 // node (i, j, k) at padded (i + q nx, j + r ny, k), x and y extended by one
 // box, so a box never wraps.  Weights, the contraction order and the
@@ -44,32 +46,23 @@ constexpr int kTI = 2, kTJ = 4, kTK = 32;    // arrival tile (x, y, z)
 // z extent sets the row stride in shared memory: 48 doubles = 384 bytes, a
 // multiple of the 128-byte bank cycle, so lanes whose stencil base moved one
 // row in x or y keep their banks (40 doubles gave 3.12 wavefronts per 8-byte
-// load, 48 gives 2.33).  Order 6: 9 x 10 x 48 doubles = 34.6 KB, so the two
-// boxes of a block let three blocks share an SM (80 registers, some spill);
-// measured at 256^3 (trace+gather per step): 10 x 12 boxes at two blocks per
-// SM 10.64 ms, 9 x 10 at three 9.86 ms, the L1 gather 10.73 ms.  Order 4:
-// 7 x 9 x 48 (24.2 KB) at four blocks per SM, as the L1 kernel runs.
-#ifndef SLC_TMA_BOX_X
-#define SLC_TMA_BOX_X 9
-#endif
-#ifndef SLC_TMA_BOX_Y
-#define SLC_TMA_BOX_Y 10
-#endif
-#ifndef SLC_TMA_MIN_BLOCKS
-#define SLC_TMA_MIN_BLOCKS 3
-#endif
-#ifndef SLC_TMA_O4_MIN_BLOCKS
-#define SLC_TMA_O4_MIN_BLOCKS 4
-#endif
+// load, 48 gives 2.33).  Order 6 (k_sl_tma_seq, one box per block): 10 x 12
+// x 48 doubles = 46 KB at four blocks per SM (64 registers, some spill).
+// Measured at 256^3, trace+gather per step: two boxes per block, 10 x 12 at
+// two blocks per SM 10.64 ms, 9 x 10 at three 9.88 ms; one box, 9 x 10 at
+// three 10.00, at four 9.52, at five 9.71, 10 x 12 at four 9.62 ms (and at
+// trajectory CFL 3, 128^3: 1.55 against 1.37 ms, the larger box staging 97 %
+// of the far feet instead of 63 %); the L1 gather 10.76 ms.  Order 4
+// (k_sl_tma, both boxes at once): 7 x 9 x 48 (24.2 KB) at four blocks.
 template <int O>
 struct Box {
-    static constexpr int X = O == 4 ? 7 : SLC_TMA_BOX_X;
-    static constexpr int Y = O == 4 ? 9 : SLC_TMA_BOX_Y;
+    static constexpr int X = O == 4 ? 7 : 10;
+    static constexpr int Y = O == 4 ? 9 : 12;
     static constexpr int Z = 48;
     static constexpr int elems = X * Y * Z;
     static constexpr size_t bytes = (size_t)elems * sizeof(double);
-    static constexpr size_t smem = 2 * bytes + 128;  // + alignment slack (boxes start on 128 bytes)
-    static constexpr int min_blocks = O == 4 ? SLC_TMA_O4_MIN_BLOCKS : SLC_TMA_MIN_BLOCKS;
+    static constexpr size_t smem = 2 * bytes + 128;  // both boxes + alignment slack (128-byte starts)
+    static constexpr int min_blocks = 4;
 };
 // the padded copies' halo: the largest box
 constexpr int kBX = Box<6>::X > Box<4>::X ? Box<6>::X : Box<4>::X;
@@ -273,6 +266,142 @@ __global__ void __launch_bounds__(kThreads, Box<O>::min_blocks)
     }
 }
 
+// The same gather with one box buffer (the order-6 form): the near foot is
+// traced, located, staged and gathered, then the far foot, so a thread holds
+// one foot's state at a time and a block one box; more blocks share an SM,
+// and the box can be larger.
+
+__device__ __forceinline__ void block_minmax3(int *red, bool act, int a, int b, int c)
+{
+    const int v[3] = {a, b, c};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int lo = __reduce_min_sync(0xffffffffu, act ? v[q] : INT_MAX);
+        const int hi = __reduce_max_sync(0xffffffffu, act ? v[q] : INT_MIN);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&red[2 * q], lo);
+            atomicMax(&red[2 * q + 1], hi);
+        }
+    }
+}
+
+template <int O>
+__device__ __forceinline__ bool box_fits(const int *r, int i0, int j0, const SlcParams &P, int &X0, int &Y0,
+                                         int &Z0)
+{
+    const bool fit = r[0] <= r[1] && r[1] - r[0] + O <= Box<O>::X && r[3] - r[2] + O <= Box<O>::Y &&
+                     r[5] + O - (r[4] & ~1) <= Box<O>::Z;
+    X0 = Y0 = Z0 = 0;
+    if (fit) {
+        X0 = (i0 + r[0]) % P.nx;
+        if (X0 < 0) X0 += P.nx;
+        Y0 = (j0 + r[2]) % P.ny;
+        if (Y0 < 0) Y0 += P.ny;
+        Z0 = r[4] & ~1;
+    }
+    return fit;
+}
+
+template <int C, int O>
+__global__ void __launch_bounds__(kThreads, Box<O>::min_blocks)
+    k_sl_tma_seq(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3 M, const double *__restrict__ fn,
+                 const double *__restrict__ fnm1, double dt, double *__restrict__ out,
+                 unsigned long long *nclamp, unsigned long long *stats, const __grid_constant__ CUtensorMap tmN,
+                 const __grid_constant__ CUtensorMap tmM)
+{
+    extern __shared__ unsigned char smraw[];
+    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ int red[12];  // per foot: min/max of rx, ry, k0
+    __shared__ int near_lost;  // the near copy did not complete: the box is not reused
+    double *box = (double *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.z * kTI, j0 = blockIdx.y * kTJ;
+    const int k = blockIdx.x * kTK + (tid & 31);
+    const int j = j0 + ((tid >> 5) & (kTJ - 1));
+    const int i = i0 + (tid >> 7);
+    const int nzi = (C == 2) ? P.nz - 1 : P.nz;
+    const bool act = k < nzi && j < P.ny && i < P.nx;
+    const unsigned barN = smem_u32(&mbar[0]), barM = smem_u32(&mbar[1]);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            red[2 * q] = INT_MAX;
+            red[2 * q + 1] = INT_MIN;
+        }
+        near_lost = 0;
+        mbar_init(barN, 1);
+        mbar_init(barM, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    unsigned ncl = 0;
+    double xa = 0.0, ya = 0.0, za = 0.0, us0 = 0.0, vs0 = 0.0, ws0 = 0.0, xd = 0.0, yd = 0.0, zd = 0.0;
+    Foot F{};
+    if (act) {
+        arrival_point<C>(P, i, j, k, xa, ya, za);
+        first_sample<C>(P, M, i, j, k, xa, ya, za, us0, vs0, ws0);
+        trace_foot(P, M, xa, ya, za, 0.5 * dt, us0, vs0, ws0, xd, yd, zd);
+        F = locate_foot<C, O>(P, xd, yd, zd, i0, j0, ncl);
+    }
+    block_minmax3(red, act, F.rx, F.ry, F.k0);
+    __syncthreads();
+    int X0, Y0, Z0;
+    const bool fitN = box_fits<O>(red, i0, j0, P, X0, Y0, Z0);
+    if (tid == 0) {
+        // stats: [0] time-outs, [1] blocks, [2] near boxes staged, [3] far boxes staged
+        atomicAdd(stats + 1, 1ull);
+        if (fitN) {
+            atomicAdd(stats + 2, 1ull);
+            mbar_expect_tx(barN, (unsigned)Box<O>::bytes);
+            tma_load_3d(smem_u32(box), &tmN, Z0, Y0, X0, barN);
+        }
+    }
+    double ubar = 0.0;
+    if (act) {
+        const bool staged = fitN && mbar_wait(barN);
+        if (fitN && !staged) atomicAdd(stats, 1ull);
+        if (staged)
+            ubar = gather_box<C, O>(P, box, F, F.rx - red[0], F.ry - red[2], F.k0 - Z0);
+        else
+            ubar = gather_global<C, O>(P, ghost_view<double>(C, fn, P.nx, P.ny, P.nz), xd, yd, F);
+    }
+    __syncthreads();  // every thread is done with the near box
+    if (tid == 0 && fitN && !mbar_wait(barN)) {
+        atomicAdd(stats, 1ull);
+        near_lost = 1;
+    }
+    if (act) {
+        trace_foot(P, M, xa, ya, za, dt, us0, vs0, ws0, xd, yd, zd);  // half of 2 dt
+        F = locate_foot<C, O>(P, xd, yd, zd, i0, j0, ncl);
+    }
+    block_minmax3(red + 6, act, F.rx, F.ry, F.k0);
+    __syncthreads();
+    const bool fitM = !near_lost && box_fits<O>(red + 6, i0, j0, P, X0, Y0, Z0);
+    if (tid == 0 && fitM) {
+        atomicAdd(stats + 3, 1ull);
+        mbar_expect_tx(barM, (unsigned)Box<O>::bytes);
+        tma_load_3d(smem_u32(box), &tmM, Z0, Y0, X0, barM);
+    }
+    if (act) {
+        double ubb;
+        const bool staged = fitM && mbar_wait(barM);
+        if (fitM && !staged) atomicAdd(stats, 1ull);
+        if (staged)
+            ubb = gather_box<C, O>(P, box, F, F.rx - red[6], F.ry - red[8], F.k0 - Z0);
+        else
+            ubb = gather_global<C, O>(P, ghost_view<double>(C, fnm1, P.nx, P.ny, P.nz), xd, yd, F);
+        const double Rn = xy_diffusion<C>(P, fn, i, j, k);
+        const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion<C>(P, fnm1, i, j, k);
+        double res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
+        res = res + ((2.0 / 3.0) * dt) * Rh;
+        const GhostShape g = ghost_shape(C, P.nx, P.ny, P.nz);
+        out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
+    }
+    add_clamps(nclamp, ncl);
+    if (tid == 0 && fitM && !mbar_wait(barM)) atomicAdd(stats, 1ull);
+}
+
 // U* = 2 V^n - V^{n-1} at every node (ghost-shaped, node entries only) and
 // the halo-padded node copies of V^n and V^{n-1}.  One warp per padded
 // (x, y) row, lanes along z (contiguous in both layouts); the row's source
@@ -338,20 +467,38 @@ cudaError_t launch_tma_t(const SlcParams &P, const Vel3 &M, Tri fn, Tri fnm1, do
 {
     const dim3 gc((P.nz + kTK - 1) / kTK, (P.ny + kTJ - 1) / kTJ, (P.nx + kTI - 1) / kTI);
     const dim3 gw((P.nz - 1 + kTK - 1) / kTK, (P.ny + kTJ - 1) / kTJ, (P.nx + kTI - 1) / kTI);
-    // per device context, so set on every launch (a host-side attribute write)
-    cudaError_t attr = cudaFuncSetAttribute(k_sl_tma<0, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
-    if (attr == cudaSuccess)
-        attr = cudaFuncSetAttribute(k_sl_tma<1, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
-    if (attr == cudaSuccess)
-        attr = cudaFuncSetAttribute(k_sl_tma<2, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
-    if (attr != cudaSuccess) return attr;
-    const CUtensorMap *tm = (const CUtensorMap *)T.maps;
-    k_sl_tma<0, O><<<gc, kThreads, Box<O>::smem, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl, stats, tm[0], tm[3]);
-    k_sl_tma<1, O><<<gc, kThreads, Box<O>::smem, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl, stats, tm[1], tm[4]);
-    if (P.nz > 1)
-        k_sl_tma<2, O><<<gw, kThreads, Box<O>::smem, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl, stats, tm[2], tm[5]);
-    count_launches(P.nz > 1 ? 3 : 2);
-    return cudaGetLastError();
+    // the attributes are per device context, so set on every launch (a
+    // host-side attribute write)
+    if constexpr (O == 6) {  // one box per block
+        const size_t sm = Box<O>::bytes + 128;
+        cudaError_t e = cudaFuncSetAttribute(k_sl_tma_seq<0, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_sl_tma_seq<1, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_sl_tma_seq<2, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        const CUtensorMap *tq = (const CUtensorMap *)T.maps;
+        k_sl_tma_seq<0, O><<<gc, kThreads, sm, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl, stats, tq[0], tq[3]);
+        k_sl_tma_seq<1, O><<<gc, kThreads, sm, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl, stats, tq[1], tq[4]);
+        if (P.nz > 1)
+            k_sl_tma_seq<2, O><<<gw, kThreads, sm, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl, stats, tq[2], tq[5]);
+        count_launches(P.nz > 1 ? 3 : 2);
+        return cudaGetLastError();
+    } else {  // both boxes at once
+        cudaError_t attr = cudaFuncSetAttribute(k_sl_tma<0, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_sl_tma<1, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_sl_tma<2, O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Box<O>::smem);
+        if (attr != cudaSuccess) return attr;
+        const CUtensorMap *tm = (const CUtensorMap *)T.maps;
+        k_sl_tma<0, O><<<gc, kThreads, Box<O>::smem, s>>>(P, M, fn.u, fnm1.u, dt, out.u, ncl, stats, tm[0], tm[3]);
+        k_sl_tma<1, O><<<gc, kThreads, Box<O>::smem, s>>>(P, M, fn.v, fnm1.v, dt, out.v, ncl, stats, tm[1], tm[4]);
+        if (P.nz > 1)
+            k_sl_tma<2, O><<<gw, kThreads, Box<O>::smem, s>>>(P, M, fn.w, fnm1.w, dt, out.w, ncl, stats, tm[2], tm[5]);
+        count_launches(P.nz > 1 ? 3 : 2);
+        return cudaGetLastError();
+    }
 }
 
 }  // namespace
