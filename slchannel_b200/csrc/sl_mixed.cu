@@ -395,31 +395,32 @@ __global__ void __launch_bounds__(kThreads, SLC_SLM_MIN_BLOCKS)
 }
 
 // ---- the BDF2 trace+gather with TMA-staged FP32 boxes ------------------------
-// A block is 2 (x) x 4 (y) x 32 (z) arrival points, one warp per 32 z.  Every
-// thread traces both feet (the FP32 trace above); the block takes the min and
-// max of the feet's stencil bases, and where a foot's bounding box fits
-// kMBX x kMBY x kMBZ nodes one thread loads it by TMA (no multicast) from the
-// halo-padded FP32 copy of V^n (near foot) or V^{n-1} (far foot) onto an
-// mbarrier.  A box row is 64 floats = 256 bytes, two whole bank cycles, so a
-// lane whose stencil base moved one row in x or y (the floor of its foot
-// coordinate flipped) keeps its bank.  Blocks whose feet spread wider gather
-// through L1 from the same padded copies.  Weights, the contraction order and
-// the FP64 mean term are gather_foot32's, so the results equal k_sl_mixed's.
+// A block is 2 (x) x 4 (y) x 32 (z) arrival points, one warp per 32 z, with
+// one box buffer.  Its threads trace the near foot (the FP32 trace above);
+// the block takes the min and max of the feet's stencil bases, and where the
+// bounding box fits kMBX x kMBY x kMBZ nodes one thread loads it by TMA (no
+// multicast) from the halo-padded FP32 copy of V^n onto an mbarrier and the
+// threads gather from it; then the far foot goes through the same buffer
+// from the copy of V^{n-1}.  A box row is 64 floats = 256 bytes, two whole
+// bank cycles, so a lane whose stencil base moved one row in x or y (the
+// floor of its foot coordinate flipped) keeps its bank.  Blocks whose feet
+// spread wider gather through L1 from the same padded copies.  Weights, the
+// contraction order and the FP64 mean term are gather_foot32's, so the
+// results equal k_sl_mixed's.
 constexpr int kMTI = 2, kMTJ = 4, kMTK = 32;   // arrival tile (x, y, z)
-// staged box (x, y, z) in nodes: 25.6 KB, so the two boxes of a block let
-// four blocks share an SM (at 64 registers), as the L1 kernel runs.  Measured
-// at 256^3 (mixed trace+gather per step): boxes 12 deep in y at three
-// blocks per SM 6.56 ms, 10 deep at three 6.49 ms, 10 deep at four 6.02 ms;
-// two blocks per SM (128 registers, no spill) 7.98 ms.
+// staged box (x, y, z) in nodes: 30.7 KB, five blocks per SM (48 registers).
+// Measured at 256^3 (mixed trace+gather per step): both feet's boxes at
+// once, 10 x 10 at four blocks per SM 6.04 ms (10 x 12 at three 6.56, two
+// blocks 7.98); one buffer, 10 x 10 at four 6.12, at five 5.94, at six 6.11,
+// 10 x 12 at five 5.99 ms, kept for the room it leaves feet that spread.
 #ifndef SLC_SLMT_BOX_Y
-#define SLC_SLMT_BOX_Y 10
+#define SLC_SLMT_BOX_Y 12
 #endif
 constexpr int kMBX = 10, kMBY = SLC_SLMT_BOX_Y, kMBZ = 64;
 constexpr int kMBoxElems = kMBX * kMBY * kMBZ;
 constexpr size_t kMBoxBytes = (size_t)kMBoxElems * sizeof(float);
-constexpr size_t kMSmemBytes = 2 * kMBoxBytes + 128;  // + alignment slack (boxes start on 128 bytes)
 #ifndef SLC_SLMT_MIN_BLOCKS
-#define SLC_SLMT_MIN_BLOCKS 4
+#define SLC_SLMT_MIN_BLOCKS 5
 #endif
 static_assert(kMTI * kMTJ * kMTK == kThreads, "one thread per arrival point");
 static_assert((kMBZ * sizeof(float)) % 128 == 0, "box rows of whole bank cycles");
@@ -507,19 +508,51 @@ __device__ __forceinline__ double gather_box_m32(const SlcParams &P, const Mixed
     return (double)acc + mean;
 }
 
+
+__device__ __forceinline__ void block_minmax3_m(int *red, bool act, int a, int b, int c)
+{
+    const int v[3] = {a, b, c};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int lo = __reduce_min_sync(0xffffffffu, act ? v[q] : INT_MAX);
+        const int hi = __reduce_max_sync(0xffffffffu, act ? v[q] : INT_MIN);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&red[2 * q], lo);
+            atomicMax(&red[2 * q + 1], hi);
+        }
+    }
+}
+
+template <int O>
+__device__ __forceinline__ bool mbox_fits(const int *r, int i0, int j0, const SlcParams &P, int &X0, int &Y0,
+                                          int &Z0)
+{
+    const bool fit = r[0] <= r[1] && r[1] - r[0] + O <= kMBX && r[3] - r[2] + O <= kMBY &&
+                     r[5] + O - (r[4] & ~3) <= kMBZ;
+    X0 = Y0 = Z0 = 0;
+    if (fit) {
+        X0 = (i0 + r[0]) % P.nx;
+        if (X0 < 0) X0 += P.nx;
+        Y0 = (j0 + r[2]) % P.ny;
+        if (Y0 < 0) Y0 += P.ny;
+        Z0 = r[4] & ~3;
+    }
+    return fit;
+}
+
 template <int C, int O, int TO>
 __global__ void __launch_bounds__(kThreads, SLC_SLMT_MIN_BLOCKS)
     k_sl_mixed_tma(const __grid_constant__ SlcParams P, const __grid_constant__ Vel3M M,
-                   const __grid_constant__ MixedView FA, const __grid_constant__ MixedView FB,
-                   const double *__restrict__ fn, const double *__restrict__ fnm1, double dt,
-                   double *__restrict__ out, unsigned long long *nclamp, unsigned long long *stats,
-                   const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB)
+                       const __grid_constant__ MixedView FA, const __grid_constant__ MixedView FB,
+                       const double *__restrict__ fn, const double *__restrict__ fnm1, double dt,
+                       double *__restrict__ out, unsigned long long *nclamp, unsigned long long *stats,
+                       const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB)
 {
     extern __shared__ unsigned char smraw[];
     __shared__ __align__(8) unsigned long long mbar[2];
-    __shared__ int red[12];  // per foot: min/max of rx, ry, k0
-    float *boxA = (float *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
-    float *boxB = boxA + kMBoxElems;
+    __shared__ int red[12];
+    __shared__ int near_lost;
+    float *box = (float *)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
     const int tid = threadIdx.x, lane = tid & 31;
     const int i0 = blockIdx.z * kMTI, j0 = blockIdx.y * kMTJ;
     const int k = blockIdx.x * kMTK + lane;
@@ -534,6 +567,7 @@ __global__ void __launch_bounds__(kThreads, SLC_SLMT_MIN_BLOCKS)
             red[2 * q] = INT_MAX;
             red[2 * q + 1] = INT_MIN;
         }
+        near_lost = 0;
         mbar_init(barA, 1);
         mbar_init(barB, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -542,11 +576,10 @@ __global__ void __launch_bounds__(kThreads, SLC_SLMT_MIN_BLOCKS)
 
     unsigned ncl = 0;
     Arr32 A{};
-    float ddx = 0.f, ddy = 0.f, ddz = 0.f, fdx = 0.f, fdy = 0.f, fdz = 0.f;
-    FootM32 Fn{}, Fm{};
+    float us0 = 0.f, vs0 = 0.f, ws0 = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
+    FootM32 F{};
     if (act) {
         A = arrival32<C>(P, i, j, k);
-        float us0, vs0, ws0;
         if (TO == 4) {
             sample3_32_o4(P, M, A, 0.f, 0.f, 0.f, us0, vs0, ws0);
         } else {
@@ -556,70 +589,57 @@ __global__ void __launch_bounds__(kThreads, SLC_SLMT_MIN_BLOCKS)
             vs0 = (float)v0;
             ws0 = (float)w0;
         }
-        trace_foot32<TO>(P, M, A, (float)(0.5 * dt), us0, vs0, ws0, ddx, ddy, ddz);
-        trace_foot32<TO>(P, M, A, (float)dt, us0, vs0, ws0, fdx, fdy, fdz);
-        Fn = locate_foot_m32<C, O>(P, A, ddx, ddy, ddz, i0, j0, ncl);
-        Fm = locate_foot_m32<C, O>(P, A, fdx, fdy, fdz, i0, j0, ncl);
+        trace_foot32<TO>(P, M, A, (float)(0.5 * dt), us0, vs0, ws0, dx, dy, dz);
+        F = locate_foot_m32<C, O>(P, A, dx, dy, dz, i0, j0, ncl);
     }
-    {  // block min/max of the stencil bases: warp reductions, then shared atomics
-        const int v[6] = {Fn.rx, Fn.ry, Fn.k0, Fm.rx, Fm.ry, Fm.k0};
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            const int lo = __reduce_min_sync(0xffffffffu, act ? v[q] : INT_MAX);
-            const int hi = __reduce_max_sync(0xffffffffu, act ? v[q] : INT_MIN);
-            if (lane == 0) {
-                atomicMin(&red[2 * q], lo);
-                atomicMax(&red[2 * q + 1], hi);
-            }
-        }
-    }
+    block_minmax3_m(red, act, F.rx, F.ry, F.k0);
     __syncthreads();
-    bool fit[2];
-    int X0[2] = {0, 0}, Y0[2] = {0, 0}, Z0[2] = {0, 0};
-#pragma unroll
-    for (int f = 0; f < 2; ++f) {
-        const int *r = red + 6 * f;
-        fit[f] = r[0] <= r[1] && r[1] - r[0] + O <= kMBX && r[3] - r[2] + O <= kMBY &&
-                 r[5] + O - (r[4] & ~3) <= kMBZ;
-        if (fit[f]) {  // the bases are within a few million nodes: no overflow
-            int x0 = (i0 + r[0]) % P.nx;
-            if (x0 < 0) x0 += P.nx;
-            int y0 = (j0 + r[2]) % P.ny;
-            if (y0 < 0) y0 += P.ny;
-            X0[f] = x0;
-            Y0[f] = y0;
-            Z0[f] = r[4] & ~3;  // a multiple of 4 floats: 16-byte aligned inner coordinate
-        }
-    }
+    int X0, Y0, Z0;
+    const bool fitA = mbox_fits<O>(red, i0, j0, P, X0, Y0, Z0);
     if (tid == 0) {
         // stats: [0] time-outs, [1] blocks, [2] near boxes staged, [3] far boxes staged
         atomicAdd(stats + 1, 1ull);
-        if (fit[0]) atomicAdd(stats + 2, 1ull);
-        if (fit[1]) atomicAdd(stats + 3, 1ull);
-        if (fit[0]) {
+        if (fitA) {
+            atomicAdd(stats + 2, 1ull);
             mbar_expect_tx(barA, (unsigned)kMBoxBytes);
-            tma_load_3d(smem_u32(boxA), &tmA, Z0[0], Y0[0], X0[0], barA);
-        }
-        if (fit[1]) {
-            mbar_expect_tx(barB, (unsigned)kMBoxBytes);
-            tma_load_3d(smem_u32(boxB), &tmB, Z0[1], Y0[1], X0[1], barB);
+            tma_load_3d(smem_u32(box), &tmA, Z0, Y0, X0, barA);
         }
     }
+    double ubar = 0.0;
+    unsigned none = 0;  // the clamps were counted when the feet were located
     if (act) {
-        unsigned none = 0;  // the clamps were counted when the feet were located
-        double ubar, ubb;
-        bool staged = fit[0] && mbar_wait(barA);
-        if (fit[0] && !staged) atomicAdd(stats, 1ull);
+        const bool staged = fitA && mbar_wait(barA);
+        if (fitA && !staged) atomicAdd(stats, 1ull);
         if (staged)
-            ubar = gather_box_m32<C, O>(P, FA, boxA, Fn, Fn.rx - red[0], Fn.ry - red[2], Fn.k0 - Z0[0]);
+            ubar = gather_box_m32<C, O>(P, FA, box, F, F.rx - red[0], F.ry - red[2], F.k0 - Z0);
         else
-            ubar = gather_foot32<C, O>(P, FA, A, ddx, ddy, ddz, none);
-        staged = fit[1] && mbar_wait(barB);
-        if (fit[1] && !staged) atomicAdd(stats, 1ull);
+            ubar = gather_foot32<C, O>(P, FA, A, dx, dy, dz, none);
+    }
+    __syncthreads();  // every thread is done with the near box
+    if (tid == 0 && fitA && !mbar_wait(barA)) {
+        atomicAdd(stats, 1ull);
+        near_lost = 1;
+    }
+    if (act) {
+        trace_foot32<TO>(P, M, A, (float)dt, us0, vs0, ws0, dx, dy, dz);
+        F = locate_foot_m32<C, O>(P, A, dx, dy, dz, i0, j0, ncl);
+    }
+    block_minmax3_m(red + 6, act, F.rx, F.ry, F.k0);
+    __syncthreads();
+    const bool fitB = !near_lost && mbox_fits<O>(red + 6, i0, j0, P, X0, Y0, Z0);
+    if (tid == 0 && fitB) {
+        atomicAdd(stats + 3, 1ull);
+        mbar_expect_tx(barB, (unsigned)kMBoxBytes);
+        tma_load_3d(smem_u32(box), &tmB, Z0, Y0, X0, barB);
+    }
+    if (act) {
+        double ubb;
+        const bool staged = fitB && mbar_wait(barB);
+        if (fitB && !staged) atomicAdd(stats, 1ull);
         if (staged)
-            ubb = gather_box_m32<C, O>(P, FB, boxB, Fm, Fm.rx - red[6], Fm.ry - red[8], Fm.k0 - Z0[1]);
+            ubb = gather_box_m32<C, O>(P, FB, box, F, F.rx - red[6], F.ry - red[8], F.k0 - Z0);
         else
-            ubb = gather_foot32<C, O>(P, FB, A, fdx, fdy, fdz, none);
+            ubb = gather_foot32<C, O>(P, FB, A, dx, dy, dz, none);
         const double Rn = xy_diffusion64<C>(P, fn, i, j, k);
         const double Rh = P.xy_lagged ? Rn : 2.0 * Rn - xy_diffusion64<C>(P, fnm1, i, j, k);
         double res = ubar * (4.0 / 3.0) + ubb * (-1.0 / 3.0);
@@ -628,12 +648,7 @@ __global__ void __launch_bounds__(kThreads, SLC_SLMT_MIN_BLOCKS)
         out[(size_t)(i + 1) * g.Y * g.Z + (size_t)(j + 1) * g.Z + (k + 1)] = res;
     }
     add_clamps(nclamp, ncl);
-    // no copy may still be writing this block's shared memory when it exits;
-    // a drain that gives up is counted with the other time-outs
-    if (tid == 0) {
-        if (fit[0] && !mbar_wait(barA)) atomicAdd(stats, 1ull);
-        if (fit[1] && !mbar_wait(barB)) atomicAdd(stats, 1ull);
-    }
+    if (tid == 0 && fitB && !mbar_wait(barB)) atomicAdd(stats, 1ull);
 }
 
 // ---- plane means -----------------------------------------------------------
@@ -1052,23 +1067,24 @@ cudaError_t launch_mtma_t(const SlcParams &P, const Vel3M &M, const MixedView *F
 {
     const dim3 gc((P.nz + kMTK - 1) / kMTK, (P.ny + kMTJ - 1) / kMTJ, (P.nx + kMTI - 1) / kMTI);
     const dim3 gw((P.nz - 1 + kMTK - 1) / kMTK, (P.ny + kMTJ - 1) / kMTJ, (P.nx + kMTI - 1) / kMTI);
-    // per device context, so set on every launch (a host-side attribute write)
+
+    // the attributes are per device context, so set on every launch (a
+    // host-side attribute write)
+    const size_t sm = kMBoxBytes + 128;
     cudaError_t e = cudaFuncSetAttribute(k_sl_mixed_tma<0, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kMSmemBytes);
+                                         (int)sm);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sl_mixed_tma<1, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kMSmemBytes);
+        e = cudaFuncSetAttribute(k_sl_mixed_tma<1, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sl_mixed_tma<2, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kMSmemBytes);
+        e = cudaFuncSetAttribute(k_sl_mixed_tma<2, O, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_sl_mixed_tma<0, O, TO><<<gc, kThreads, kMSmemBytes, s>>>(P, M, FA[0], FB[0], fn.u, fnm1.u, dt, out.u, ncl,
-                                                               stats, tm[0], tm[3]);
-    k_sl_mixed_tma<1, O, TO><<<gc, kThreads, kMSmemBytes, s>>>(P, M, FA[1], FB[1], fn.v, fnm1.v, dt, out.v, ncl,
-                                                               stats, tm[1], tm[4]);
+    k_sl_mixed_tma<0, O, TO><<<gc, kThreads, sm, s>>>(P, M, FA[0], FB[0], fn.u, fnm1.u, dt, out.u, ncl, stats,
+                                                      tm[0], tm[3]);
+    k_sl_mixed_tma<1, O, TO><<<gc, kThreads, sm, s>>>(P, M, FA[1], FB[1], fn.v, fnm1.v, dt, out.v, ncl, stats,
+                                                      tm[1], tm[4]);
     if (P.nz > 1)
-        k_sl_mixed_tma<2, O, TO><<<gw, kThreads, kMSmemBytes, s>>>(P, M, FA[2], FB[2], fn.w, fnm1.w, dt, out.w,
-                                                                   ncl, stats, tm[2], tm[5]);
+        k_sl_mixed_tma<2, O, TO><<<gw, kThreads, sm, s>>>(P, M, FA[2], FB[2], fn.w, fnm1.w, dt, out.w, ncl,
+                                                          stats, tm[2], tm[5]);
     count_launches(P.nz > 1 ? 3 : 2);
     return cudaGetLastError();
 }
