@@ -28,6 +28,9 @@ struct slc_ensemble {
     std::vector<slc_grid *> grids;
     std::vector<EnsInst> host_inst;
     std::vector<int> tkl;
+    // instances whose trace+gather runs as the single-grid TMA-staged launches
+    // (large enough to fill the GPU alone) instead of in the persistent kernel
+    std::vector<char> staged;
     bool bound = false;
     std::string err;
     // device copies
@@ -56,6 +59,12 @@ struct slc_ensemble {
     cudaStream_t cap = nullptr;
     cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
 };
+
+// An order-6 instance whose staged trace+gather has at least this many
+// blocks per component (a few waves of the GPU) runs it as its own launches.
+#ifndef SLC_ENS_STAGED_MIN_BLOCKS
+#define SLC_ENS_STAGED_MIN_BLOCKS 2048
+#endif
 
 namespace {
 
@@ -149,9 +158,10 @@ void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
     }
     end(e->r_bc);
     // U* = 2 V^n - V^{n-1}: 1024 elements per block
+    auto st = [&](int i) { return i < (int)e->staged.size() && e->staged[i]; };
     begin(e->r_lin);
     for (int i = 0; i < n; ++i)
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < 3 && !st(i); ++c) {
             const long long ne = (long long)e->grids[i]->ghost_elems[c];
             const int nb = (int)((ne + 1023) / 1024);
             for (int b = 0; b < nb; ++b) items.push_back({i, c, b, 0});
@@ -160,6 +170,7 @@ void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
     // trace+gather: (instance, component, x index, (y tile << 16) | z tile)
     begin(e->r_sl);
     for (int i = 0; i < n; ++i) {
+        if (st(i)) continue;
         const SlcParams &P = e->grids[i]->P;
         const int tk = 1 << e->tkl[i], tj = 256 / tk;
         for (int c = 0; c < 3; ++c) {
@@ -213,12 +224,13 @@ void build_items(slc_ensemble *e, std::vector<EnsItem> &items)
     begin(e->r_pp);
     if (e->mixed)
         for (int i = 0; i < n; ++i)
-            for (int f = 0; f < 6; ++f)
+            for (int f = 0; f < 6 && !st(i); ++f)
                 for (int b = 0; b < mixed_mean_blocks(); ++b) items.push_back({i, b, f, 0});
     end(e->r_pp);
     begin(e->r_pack);
     if (e->mixed)
         for (int i = 0; i < n; ++i) {
+            if (st(i)) continue;
             const SlcParams &P = e->grids[i]->P;
             const MixedWS &ws = e->grids[i]->mws;
             e->pack_threads = std::max(e->pack_threads,
@@ -271,6 +283,26 @@ int enqueue_step(slc_ensemble *e, int ph, cudaStream_t s)
     for (int i = 0; i < n; ++i)
         ENS_CK(cudaMemsetAsync(e->host_inst[i].ncl, 0, sizeof(unsigned long long), s), "memset");
     ENS_CK(cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned), s), "memset");
+    const int prv = ens_prev(ph);
+    for (int i = 0; i < n; ++i) {
+        if (!e->staged[i]) continue;
+        slc_grid *g = e->grids[i];
+        const EnsInst &H = e->host_inst[i];
+        const Tri a{H.lev[cur][0], H.lev[cur][1], H.lev[cur][2]}, b{H.lev[prv][0], H.lev[prv][1], H.lev[prv][2]};
+        const TriMut o{H.lev[nxt][0], H.lev[nxt][1], H.lev[nxt][2]};
+        if (e->mixed) {
+            ENS_CK(launch_mixed_prepare(g->P, a, b, Tri{nullptr, nullptr, nullptr}, g->mws, s, &g->tmx),
+                   "mixed-form pack (padded)");
+            ENS_CK(launch_sl_mixed_tma(g->P, a, b, g->mws, g->tmx, H.dt, o, H.ncl, g->dev_flags, s),
+                   "mixed trace+gather BDF2 (TMA-staged)");
+        } else {
+            ENS_CK(launch_mid_pack(g->P, a, b, TriMut{g->mid[0], g->mid[1], g->mid[2]}, g->tma, s),
+                   "U* and padded node copies");
+            ENS_CK(launch_sl_tma(g->P, a, b, Tri{g->mid[0], g->mid[1], g->mid[2]}, H.dt, o, H.ncl, g->dev_flags,
+                                 g->tma, s),
+                   "trace+gather BDF2 (TMA-staged)");
+        }
+    }
     if (e->mixed)
         ENS_CK(launch_sl_mixed_ens(I, items_at(e, e->r_sl), e->r_sl.n, ph, e->order, e->traj, e->d_queue,
                                    e->sl_grid, s),
@@ -491,6 +523,19 @@ int slc_ensemble_bind(slc_ensemble *e, double *const *lev, double *const *p, con
             I.mws = g->mws;
         }
     }
+    // the large order-6 instances gather through the single-grid staged
+    // launches (each fills the GPU alone); the rest share the persistent kernel
+    e->staged.assign(n, 0);
+    if (e->order == 6)
+        for (int i = 0; i < n; ++i) {
+            const SlcParams &P = e->grids[i]->P;
+            const long long blocks = (long long)((P.nz + 31) / 32) * ((P.ny + 3) / 4) * ((P.nx + 1) / 2);
+            if (blocks < SLC_ENS_STAGED_MIN_BLOCKS) continue;
+            bool ready = false;
+            int rs = slc_grid_ensure_staged(e->grids[i], &ready);
+            if (rs) return efail(e, rs, std::string("instance ") + std::to_string(i) + ": " + e->grids[i]->err);
+            e->staged[i] = ready ? 1 : 0;
+        }
     ENS_CK(cudaDeviceSynchronize(), "z-solve tables");
     int rc = upload_tables(e);
     if (rc) return rc;

@@ -1165,7 +1165,8 @@ cudaError_t launch_mixed_prepare_ens(const EnsInst *ins, int ninst, const EnsIte
                                      const EnsItem *pack_items, int n_pack, int pack_threads, int ph,
                                      cudaStream_t s)
 {
-    if (ninst <= 0) return cudaSuccess;
+    // no items: every instance packs its own buffers (the staged gather)
+    if (ninst <= 0 || n_pp <= 0 || n_pack <= 0) return cudaSuccess;
     k_plane_partials_ens<<<n_pp, 256, 0, s>>>(ins, pp_items, ph);
     k_plane_finish_ens<<<9 * ninst, 256, 0, s>>>(ins);
     k_pack_mixed_ens<<<n_pack, pack_threads, 0, s>>>(ins, pack_items, ph);

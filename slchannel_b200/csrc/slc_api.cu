@@ -228,6 +228,21 @@ int ensure_mixed(slc_grid *g)
 int slc_grid_ensure_mixed(slc_grid *g) { return ensure_mixed(g); }
 int slc_grid_ensure_mid(slc_grid *g) { return ensure_mid(g); }
 
+int slc_grid_ensure_staged(slc_grid *g, bool *ready)
+{
+    *ready = false;
+    int rc;
+    if (g->mixed) {
+        rc = ensure_mixed_tma(g);
+        if (!rc) *ready = g->tmx_state == 1;
+    } else {
+        rc = ensure_mid(g);
+        if (!rc) rc = ensure_tma(g);
+        if (!rc) *ready = g->tma_state == 1;
+    }
+    return rc;
+}
+
 // The BDF2 step after its trace+gather: the implicit z diffusion and the
 // projection of next (slc_step_bdf2's tail; the host step streams the rest).
 int slc_step_bdf2_tail(slc_grid *g, double *const next[3], double *p, double dt, cudaStream_t s)

@@ -73,5 +73,8 @@ struct slc_grid {
 int slc_grid_ensure_mixed(slc_grid *g);
 // Allocate the U* workspace g->mid (slc_api.cu).
 int slc_grid_ensure_mid(slc_grid *g);
+// Allocate what the handle's TMA-staged BDF2 gather needs (padded copies,
+// tensor maps); *ready tells whether the grid can use it (slc_api.cu).
+int slc_grid_ensure_staged(slc_grid *g, bool *ready);
 // zsolve + projection of slc_step_bdf2 after its trace+gather (slc_api.cu).
 int slc_step_bdf2_tail(slc_grid *g, double *const next[3], double *p, double dt, cudaStream_t s);
