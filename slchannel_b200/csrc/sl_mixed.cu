@@ -425,6 +425,27 @@ constexpr size_t kMBoxBytes = (size_t)kMBoxElems * sizeof(float);
 static_assert(kMTI * kMTJ * kMTK == kThreads, "one thread per arrival point");
 static_assert((kMBZ * sizeof(float)) % 128 == 0, "box rows of whole bank cycles");
 
+#ifndef SLC_SLMT_F32X2  // packed FP32x2 FMAs in the box gather: 5.99 -> 5.81 ms per step at 256^3
+#define SLC_SLMT_F32X2 1
+#endif
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void unpack_f32x2(unsigned long long v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
+                                                       unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
 // A foot located for the staged gather: x and y stencil bases (unwrapped,
 // relative to the tile origin), their fractions, the clamped height and the
 // z base; split32's and gather_foot32's arithmetic without the wrap.
@@ -489,6 +510,29 @@ __device__ __forceinline__ double gather_box_m32(const SlcParams &P, const Mixed
     }
     const float *b = box + (ox * kMBY + oy) * kMBZ + oz;
     float acc = 0.f;
+#if SLC_SLMT_F32X2
+    // two rows' z contractions per packed FP32x2 FMA (each lane an IEEE fma,
+    // so the sums equal the scalar ones)
+    unsigned long long w2[O];
+#pragma unroll
+    for (int k = 0; k < O; ++k) w2[k] = pack_f32x2(wz[k], wz[k]);
+#pragma unroll
+    for (int i = 0; i < O; ++i) {
+        float accy = 0.f;
+#pragma unroll
+        for (int j = 0; j < O; j += 2) {
+            const float *r0 = b + (i * kMBY + j) * kMBZ, *r1 = r0 + kMBZ;
+            unsigned long long a2 = 0ull;  // (+0, +0)
+#pragma unroll
+            for (int k = 0; k < O; ++k) a2 = fma_f32x2(w2[k], pack_f32x2(r0[k], r1[k]), a2);
+            float z0, z1;
+            unpack_f32x2(a2, z0, z1);
+            accy = fmaf(wy[j], z0, accy);
+            accy = fmaf(wy[j + 1], z1, accy);
+        }
+        acc = fmaf(wx[i], accy, acc);
+    }
+#else
 #pragma unroll
     for (int i = 0; i < O; ++i) {
         float accy = 0.f;
@@ -502,6 +546,7 @@ __device__ __forceinline__ double gather_box_m32(const SlcParams &P, const Mixed
         }
         acc = fmaf(wx[i], accy, acc);
     }
+#endif
     double mean = 0.0;
 #pragma unroll
     for (int k = 0; k < O; ++k) mean = fma((double)wz[k], __ldg(F.mean + f.k0 + k), mean);
